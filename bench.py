@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark: SparsePauliVector propagation throughput (terms/s, rotate+merge+clip).
+
+Workload (default): the 8x8-lattice circuit (N=64): observable mean Z (64 terms,
+coefficient 1/64), 20 Trotter layers of RZZ(0.3) on the 112 edges (rows, then
+columns) followed by RX(0.25) on all 64 sites, a depolarizing channel p=1e-3
+after each layer, CompositeTruncation(CoeffTruncation(1e-5), WeightTruncation(12))
+at window 1.  One step = the whole 3,520-rotation evolution from the observable
+plus <0...0|O|0...0>.  terms/s = sum over rotations of the live terms entering
+the rotation, divided by the step time.
+
+Arms:
+  --impl ours       (default) libpauliprop on the GPU.  `value`: device time of K
+                    steps (CUDA events on the engine's stream, input resident in
+                    HBM).  `e2e`: the same steps through the public API with host
+                    buffers (pinned upload, evolve, download of the final term
+                    set and the expectation value) timed by the host clock.
+  --impl reference  the reference algorithm on the host cores: the C restatement
+                    of the reference's CPU path (oracle/, "port"), one worker
+                    process per host thread, each timing one Trotter layer from
+                    the layer-10 state (a bounded sample of the same workload).
+Multi-GPU (torchrun, N > 1): every rank runs an independent replica of the
+workload (the path does not shard at this size); value = all ranks' terms over
+the slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "paulioperators.jl_b200"))
+
+BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
+SNAP_LAYER = 10                      # CPU-baseline sample: layer 11 from the layer-10 state
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["lattice64", "chain20", "graph127"], default="lattice64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-workers", type=int, default=0, help="reference arm worker processes (0: all host threads)")
+    return ap.parse_args()
+
+
+def workload(name):
+    from pauliprop import circuits
+    return {"lattice64": circuits.lattice64, "chain20": circuits.chain20,
+            "graph127": circuits.random_graph127}[name]()
+
+
+def strategy_of(w):
+    import pauliprop as pp
+    parts = [pp.CoeffTruncation(w.thresh)]
+    if w.wmax:
+        parts.append(pp.WeightTruncation(w.wmax))
+    return pp.CompositeTruncation(*parts)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+            sm = [float(r[1]) for r in rows]
+            mx = max(float(r[2]) for r in rows)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def dist_init(backend):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def reduce_max(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def _oracle_layer_sample(wname, snap_layer, reps, q=None):
+    """Worker: build the snap_layer state on the CPU oracle, then time `reps` evolutions of
+    the next layer from copies of it.  Returns [(terms_in, seconds), ...]."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    import pauliprop as pp
+    w = workload(wname)
+    f = tuple(pp.compile_filter(strategy_of(w)))
+    kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
+    v = orc.OracleSPV.from_terms(w.N, w.observable)
+    gens = [(p.z, p.x) for p in w.layer]
+    for _ in range(snap_layer):
+        v.evolve(gens, w.angles, window=1, strict=f)
+        if kind is not None:
+            v.channel(kind, [w.channel[1]])
+    out = []
+    for _ in range(reps):
+        s = v.copy()
+        n0 = len(s)
+        t0 = time.perf_counter()
+        _, ctr = s.evolve(gens, w.angles, window=1, strict=f, nwin=len(gens))
+        if kind is not None:
+            s.channel(kind, [w.channel[1]])
+        dt = time.perf_counter() - t0
+        terms_in = n0 + int(ctr[2][:-1].sum())
+        out.append((terms_in, dt))
+    if q is not None:
+        q.put(out)
+    return out
+
+
+def cpu_baseline_from_snapshot(g_arrays, w, gens_layer):
+    """Single-thread oracle timing of one layer from a GPU snapshot (identical state)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    import pauliprop as pp
+    z, x, c = g_arrays
+    f = tuple(pp.compile_filter(strategy_of(w)))
+    kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
+    v = orc.OracleSPV(w.N, max(16, 2 * len(c)), max(16, 2 * len(c)))
+    v.upload(z, x, c)
+    n0 = len(v)
+    t0 = time.perf_counter()
+    _, ctr = v.evolve(gens_layer, w.angles, window=1, strict=f, nwin=len(gens_layer))
+    if kind is not None:
+        v.channel(kind, [w.channel[1]])
+    dt = time.perf_counter() - t0
+    return n0 + int(ctr[2][:-1].sum()), dt, v
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    ws, rank, local = dist_init("gloo")
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    nthreads = args.ref_workers or os.cpu_count() or 1
+    q = ctx.Queue()
+    reps = args.warmup + args.steps
+    procs = [ctx.Process(target=_oracle_layer_sample, args=(args.workload, SNAP_LAYER, reps, q))
+             for _ in range(nthreads)]
+    for p in procs:
+        p.start()
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    # per step: aggregate throughput of all workers (timed steps only)
+    per_step = []
+    for s in range(args.warmup, reps):
+        per_step.append(sum(r[s][0] / r[s][1] for r in res))
+    value = statistics.median(per_step)
+    w = workload(args.workload)
+    terms_in = res[0][args.warmup][0]
+    line = {
+        "metric": "terms/s rotate+merge+clip", "value": value, "unit": "terms/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * terms_in / (value / nthreads), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded circuit)", "impl": "reference",
+        "config": {"workload": f"{w.name} layer {SNAP_LAYER + 1} from the layer-{SNAP_LAYER} state",
+                   "N": w.N, "rotations_per_sample": len(w.layer), "threads": nthreads},
+        "cpu_baseline": {"value": value, "unit": "terms/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{w.name}: one Trotter layer ({len(w.layer)} rotations + channel) "
+                                   f"from the layer-{SNAP_LAYER} state, per worker process"},
+        "e2e": {"value": value, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    ws, rank, local = dist_init("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import pauliprop as pp
+
+    w = workload(args.workload)
+    strat = strategy_of(w)
+    gens, angs = w.generators()
+    ch = (w.channel[0], w.channel[1], None) if w.channel else None
+    per = len(w.layer)
+    nw = pp.nwords(w.N)
+    B = BYTES_PER_TERM[nw]
+    # reference sizing of SparsePauliVector(O::PauliSum) for the observable
+    live_cap = max(16, math.ceil(2.0 * len(w.observable)))
+    ps = pp.PauliSum(w.N)
+    for z, x, c in w.observable:
+        ps[(z, x)] = c
+    obs_z, obs_x = pp.pack_keys(w.N, list(ps.keys()))
+    obs_c = np.array(list(ps.values()), dtype=np.float64)
+    order = np.lexsort(tuple(obs_x[:, k] for k in range(nw - 1, -1, -1)) + tuple(obs_z[:, k] for k in range(nw - 1, -1, -1)))
+    obs_z, obs_x, obs_c = obs_z[order], obs_x[order], obs_c[order]
+    dz = torch.from_numpy(obs_z.copy()).to(dev)
+    dx = torch.from_numpy(obs_x.copy()).to(dev)
+    dc = torch.from_numpy(obs_c.copy()).to(dev)
+
+    g = pp.SparsePauliVector(w.N, live_cap, live_cap)
+    stream = torch.cuda.ExternalStream(g.stream(), device=dev)
+
+    def upload_dev():
+        pp.spv.check(pp.spv.lib.pp_upload(g._h, dz.data_ptr(), dx.data_ptr(), dc.data_ptr(), len(obs_c), 1))
+
+    def one_step(stats=None, profile=False):
+        upload_dev()
+        _, e = pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0,
+                          return_expectation=True, stats=stats, profile=profile)
+        return e
+
+    # warm-up
+    for _ in range(args.warmup):
+        one_step()
+    st = {}
+    one_step(stats=st)
+    terms_in = st["terms_in"]
+    launches = int(st["launches"])
+
+    # timed region (device time on the engine's stream)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        expect = None
+        for _ in range(args.steps):
+            expect = one_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    t = e0.elapsed_time(e1) * 1e-3
+    t = reduce_max(t, ws, dev)
+    total_terms = reduce_sum(terms_in * args.steps, ws, dev)
+    value = total_terms / t
+
+    # e2e through the public API with host buffers
+    hz = torch.from_numpy(obs_z.copy()).pin_memory()
+    hx = torch.from_numpy(obs_x.copy()).pin_memory()
+    hc = torch.from_numpy(obs_c.copy()).pin_memory()
+    nfin = len(g)
+    oz = torch.empty((max(nfin, 1), nw), dtype=torch.uint64).pin_memory() if hasattr(torch, "uint64") else None
+    h2d = d2h = 0
+    te = []
+    for _ in range(args.steps):
+        if ws > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        pp.spv.check(pp.spv.lib.pp_upload(g._h, hz.data_ptr(), hx.data_ptr(), hc.data_ptr(), len(obs_c), 1))
+        pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0)
+        n_out = len(g)
+        zf = np.empty((n_out, nw), dtype=np.uint64)
+        xf = np.empty((n_out, nw), dtype=np.uint64)
+        cf = np.empty(n_out, dtype=np.float64)
+        m = pp.spv.c_int64()
+        pp.spv.check(pp.spv.lib.pp_download(g._h, zf.ctypes.data, xf.ctypes.data, cf.ctypes.data, n_out,
+                                            pp.spv.byref(m)))
+        ev = pp.expectation_value(g, 0)
+        te.append(time.perf_counter() - t0)
+        h2d = obs_z.nbytes + obs_x.nbytes + obs_c.nbytes + len(gens) * (2 * 8 * nw + 16)
+        d2h = zf.nbytes + xf.nbytes + cf.nbytes + 8
+    t_e2e = reduce_max(sum(te), ws, dev)
+    e2e_value = total_terms / t_e2e
+
+    # profiled pass: per-kernel device time for the roofline of the merge kernel
+    sp = {}
+    one_step(stats=sp, profile=True)
+    merge_bytes = B * (sp["merge_in"] + sp["merge_out"])          # B*(n + a + m) per launch, summed
+    achieved = merge_bytes / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
+    pipe_bytes = B * (sp["terms_in"] + sp["merge_out"])          # B*(n + m) per rotation, summed
+    hbm, src = peaks()
+
+    # CPU baseline on an identical snapshot (rank 0 at N=1)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and w.layers > SNAP_LAYER:
+        upload_dev()
+        pp.evolve_(g, w.layer * SNAP_LAYER, w.angles * SNAP_LAYER, truncation=strat, channel=ch,
+                   channel_every=per if ch else 0)
+        snap = g.to_arrays()
+        ti_cpu, dt_cpu, vorc = cpu_baseline_from_snapshot(snap, w, [(p.z, p.x) for p in w.layer])
+        # same sample on the GPU, and its result against the oracle's
+        g.upload(*snap, sorted=True)
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        st2 = {}
+        pp.evolve_(g, w.layer, w.angles, truncation=strat, channel=ch, stats=st2)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        gz_, gx_, gc_ = g.to_arrays()
+        oz_, ox_, oc_ = vorc.arrays()
+        same = bool(np.array_equal(gz_, oz_) and np.array_equal(gx_, ox_)
+                    and np.abs(gc_ - oc_).max(initial=0.0) <= 1e-12 * max(1.0, np.abs(oc_).max(initial=1.0)))
+        cpu = {"value": ti_cpu / dt_cpu, "unit": "terms/s", "cores": 1, "kind": "port",
+               "sample": f"{w.name} layer {SNAP_LAYER + 1} ({len(w.layer)} rotations + channel) from the "
+                         f"GPU's layer-{SNAP_LAYER} state ({len(snap[2])} terms), C restatement of the "
+                         f"reference path, 1 thread",
+               "gpu_same_sample_terms_per_s": st2["terms_in"] / (s0.elapsed_time(s1) * 1e-3),
+               "gpu_matches_oracle_on_sample": same}
+
+    if rank == 0:
+        line = {
+            "metric": "terms/s rotate+merge+clip", "value": value, "unit": "terms/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuit)",
+            "config": {"workload": f"{w.name}: N={w.N}, {w.layers} layers x {per} rotations, "
+                                   f"thresh {w.thresh}, wmax {w.wmax}, channel {w.channel}",
+                       "terms_in_per_step": terms_in, "peak_terms": st["peak"],
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "no flush: working set exceeds L2 at peak; the step re-creates its input"},
+            "expectation": expect,
+            "e2e": {"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "kernel": "k_merge<1,0> (merge + reduce-by-key + filter + channel + compaction)",
+                         "peak_source": src,
+                         "pipeline_frac": pipe_bytes / (sp["t_rotate"] + sp["t_merge"] + sp["t_partition"]) / 1e9 / hbm,
+                         "t_merge_s": sp["t_merge"], "t_rotate_s": sp["t_rotate"],
+                         "t_partition_commit_s": sp["t_partition"]},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,154 @@
+/*
+ * pauliprop — B200-native (sm_100a) SparsePauliVector propagation engine.
+ *
+ * C ABI of libpauliprop.so.  Every entry point is a drop-in for one method of
+ * PauliOperators.jl's SparsePauliVector propagation path; the comment above
+ * each declaration names the reference interface it replaces (file:line in
+ * the PauliOperators.jl source tree).  Plain pointers and sizes only: a Julia
+ * `ccall`, a Python `ctypes` or a C caller binds it directly.
+ *
+ * Word layout: z and x are arrays of the reference's packed word type
+ * (_word_type, src/type_SparsePauliVector.jl:23-26): one uint64 per term for
+ * N <= 64, one 16-byte little-endian UInt128 (low word first) per term for
+ * 65 <= N <= 128 — byte-identical to Julia's Vector{UInt64}/Vector{UInt128}.
+ * Coefficients are Float64 (T = Float64, the engine's real coefficient type).
+ * Term arrays stay in device memory between calls; host buffers are touched
+ * only by pp_upload / pp_download / the small argument arrays.
+ *
+ * Threading: one CUDA stream per handle; a handle is not re-entrant, distinct
+ * handles are independent.  Calls that return data synchronize.
+ * All entry points return a pp_status; pp_last_error() gives the message
+ * (thread-local).
+ */
+#ifndef PAULIPROP_H
+#define PAULIPROP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PP_OK = 0,
+    PP_ARGUMENT_ERROR = 1,      /* Julia ArgumentError (channels.jl:16-27, 225-226; spv_evolve.jl:321, 327-330) */
+    PP_DIMENSION_MISMATCH = 2,  /* Julia DimensionMismatch (spv_evolve.jl:319-320) */
+    PP_ERROR_EXCEPTION = 3,     /* Julia ErrorException (type_SparsePauliVector.jl:25, 145-147; check_spv) */
+    PP_OUT_OF_MEMORY = 4,
+    PP_DEVICE_ERROR = 5,        /* CUDA runtime error */
+    PP_TIMEOUT = 6,             /* a bounded device-side wait gave up */
+    PP_NOT_IMPLEMENTED = 7      /* strategy without a GPU path (no CPU fallback exists) */
+} pp_status;
+
+typedef struct pp_spv pp_spv;
+
+/* Byte-identical to the isbits MergeFilter (spv_kernels.jl:33-42); sentinels
+ * INT64_MAX for disabled weight caps and negative thresholds for disabled
+ * coefficient criteria, as in NOFILTER (spv_kernels.jl:44-45). */
+typedef struct {
+    int64_t wmax, xwmax, mwmax;
+    double thresh, alpha_w, dthresh_w, alpha_xw, dthresh_xw;
+} pp_filter;
+
+/* WindowCounters (spv_evolve.jl:149-161); arrays of length nwin, caller-owned.
+ * t_rotate / t_merge are device time in seconds (CUDA events). */
+typedef struct {
+    int64_t nwin;
+    int64_t *terms_created, *merge_in, *merge_out, *early_merges;
+    double *t_rotate, *t_merge;
+} pp_counters;
+
+/* Keyword arguments of the sequence evolve! (spv_evolve.jl:312-318). */
+typedef struct {
+    int64_t window;               /* window = 1 (default) */
+    const pp_filter *strict;      /* truncation (compiled); NULL = NoTruncation */
+    const pp_filter *local;       /* local_truncation; NULL = NoTruncation */
+    int32_t strict_kind;          /* 0 compiled MergeFilter, 1 AdaptiveTruncation (PP_NOT_IMPLEMENTED) */
+    int32_t corr_kind;            /* 0 NoCorrection, 1 EnergyCorrection (truncation.jl:255-266) */
+    int64_t adapt_max_terms;
+    double adapt_min_thresh;
+    const void *ket;              /* EnergyCorrection ket: one word (type as z/x) */
+    double *corr_energy;          /* in/out: accumulated_energy (EnergyCorrection) */
+    pp_counters *counters;        /* nullable */
+    int32_t chan_kind;            /* -1: none. 0..4: channel applied after the last rotation,
+                                     fused into its merge (see pp_channel) */
+    int32_t pad;
+    double chan_prm[3];
+    const void *chan_mask;        /* NULL: all qubits */
+    double *expect_out;           /* nullable: <0...0|O|0...0> of the final state (fused reduction) */
+    int64_t chan_every;           /* > 0: apply the channel after every chan_every-th rotation
+                                     (a layer loop "evolve!(v, layer...); channel!(v, p)" in one call) */
+    double *stats_out;            /* nullable, PP_STATS_LEN doubles: see PP_STAT_* */
+    int32_t profile;              /* 1: time the rotate and merge kernels with CUDA events (stats) */
+    int32_t pad2;
+} pp_evolve_opts;
+
+/* stats_out layout (sums over the call's rotations). */
+#define PP_STAT_TERMS_IN 0        /* live terms entering each rotation (terms/s numerator) */
+#define PP_STAT_CREATED 1         /* sin branches appended */
+#define PP_STAT_MERGE_IN 2        /* merge inputs (live + appended) */
+#define PP_STAT_MERGE_OUT 3       /* merge survivors */
+#define PP_STAT_PEAK 4            /* largest live count after a merge */
+#define PP_STAT_EARLY 5           /* early (capacity-forced) merges */
+#define PP_STAT_T_ROTATE 6        /* seconds in classify/scan/permute kernels (profile = 1) */
+#define PP_STAT_T_MERGE 7         /* seconds in the merge kernel alone (profile = 1) */
+#define PP_STAT_LAUNCHES 8        /* kernels launched by the call */
+#define PP_STAT_T_PARTITION 9     /* seconds in partition + commit kernels (profile = 1) */
+#define PP_STATS_LEN 16
+
+/* _alloc_spv (type_SparsePauliVector.jl:94-104) / SparsePauliVector(N, T; capacity)
+ * (type_SparsePauliVector.jl:138-141).  append_cap is the reference's logical
+ * append capacity, which drives the early-merge rule (spv_evolve.jl:356-362).
+ * N > 128 -> PP_ERROR_EXCEPTION (type_SparsePauliVector.jl:25). */
+int pp_create(int32_t N, int64_t live_cap, int64_t append_cap, pp_spv **out);
+/* Finalizer of the Julia shim. */
+int pp_destroy(pp_spv *h);
+/* Constructor fill + _sort_live! (type_SparsePauliVector.jl:167-188).  sorted != 0:
+ * input already strictly increasing (skip the device sort).  Keys must be unique. */
+int pp_upload(pp_spv *h, const void *z, const void *x, const double *c, int64_t n, int32_t sorted);
+/* PauliSum(v) gather (type_SparsePauliVector.jl:212-221): copies min(n, cap) terms
+ * to the caller's buffers (host or device pointers) and returns n. */
+int pp_download(pp_spv *h, void *z, void *x, double *c, int64_t cap, int64_t *n);
+/* length(v) (type_SparsePauliVector.jl:363). */
+int pp_length(pp_spv *h, int64_t *n);
+/* copy(v) (type_SparsePauliVector.jl:249-254). */
+int pp_copy(pp_spv *h, pp_spv **out);
+/* evolve!(O, G, θ) (spv_evolve.jl:228-236): one rotation, NOFILTER. */
+int pp_evolve1(pp_spv *h, const void *gz, const void *gx, double cos_theta, double sin_theta);
+/* evolve!(O, generators, angles; window, truncation, local_truncation, correction,
+ * counters) (spv_evolve.jl:312-387).  gz/gx: L packed generator words; cosv/sinv:
+ * host-computed cos(θ_i), sin(θ_i) (spv_evolve.jl:341-342). */
+int pp_evolve(pp_spv *h, const void *gz, const void *gx, const double *cosv, const double *sinv,
+              int64_t L, const pp_evolve_opts *opts);
+/* coeff_clip! / weight_clip! / x_weight_clip! / majorana_weight_clip! /
+ * weight_damped_clip! / x_weight_damped_clip! and the compilable truncate!
+ * (spv_evolve.jl:13-26, 59-65) -> _compact_spv! (spv_kernels.jl:395-408). */
+int pp_compact(pp_spv *h, const pp_filter *f);
+/* _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114). */
+int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh);
+/* depolarizing_channel! (channels.jl:223-232, kind 0), dephasing_channel! (234-243, 1),
+ * bit_flip_channel! (245-254, 2), bit_phase_flip_channel! (256-265, 3),
+ * pauli_channel! (203-221, 4).  prm: p, or pX,pY,pZ for kind 4.  qubit_mask: one
+ * word (NULL = all qubits) as _spv_mask (channels.jl:200-201). */
+int pp_channel(pp_spv *h, int32_t kind, const double *prm, const void *qubit_mask);
+/* expectation_value(v, ::Ket) (spv_evolve.jl:133-134) -> _expectation_spv
+ * (spv_kernels.jl:441-452).  ket: one word. */
+int pp_expect_ket(pp_spv *h, const void *ket, double *out);
+/* check_spv (type_SparsePauliVector.jl:263-278): *ok = 1 if live keys are strictly
+ * increasing and within capacity. */
+int pp_check(pp_spv *h, int32_t *ok);
+/* The handle's CUDA stream (cudaStream_t), for callers that time with events. */
+int pp_stream(pp_spv *h, void **stream);
+/* Bytes of device memory held by the handle. */
+int pp_device_bytes(pp_spv *h, int64_t *bytes);
+/* lambda^k for k = 0..kmax with the compensated integer power used by the channel
+ * tables (the algorithm of Julia's Float64^Integer). Host-only helper. */
+int pp_power_table(double lambda, int32_t kmax, double *out);
+/* Message of the last failing call on this thread. */
+const char *pp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAULIPROP_H */

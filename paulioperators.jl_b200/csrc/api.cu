@@ -1,0 +1,979 @@
+// libpauliprop: C ABI (include/pauliprop.h) over the sm_100a kernels.
+//
+// A handle owns every device buffer of one SparsePauliVector (live + scratch
+// term sets, permutation / merge workspaces, the append and sort buffers of the
+// general path) and one CUDA stream.  The live term count, the live/scratch
+// parity and the rotation cursor live in device memory (DevState), so a whole
+// sequence of window-1 rotations is launched without host round trips; the host
+// reads the state back only at chunk boundaries to grow buffers when a kernel
+// flagged that the next merge would not fit (it then resumes at the rotation
+// that stopped, which is result-invariant like the reference's _grow_live!
+// retry, spv_kernels.jl:377-386).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pauliprop.h"
+#include "kernels_general.cuh"
+
+using namespace pp;
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+extern "C" const char *pp_last_error(void) { return g_err.c_str(); }
+
+#define CU(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            return fail(e_ == cudaErrorMemoryAllocation ? PP_OUT_OF_MEMORY : PP_DEVICE_ERROR, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));             \
+        }                                                                                \
+    } while (0)
+#define TRY(call)                     \
+    do {                              \
+        int r_ = (call);              \
+        if (r_ != PP_OK) return r_;   \
+    } while (0)
+
+static const pp_filter NOFILTER_H = {INT64_MAX, INT64_MAX, INT64_MAX, -1.0, 0.0, -1.0, 0.0, -1.0};
+static constexpr int CHUNK_ROT = 32;   // rotations launched between state read-backs
+
+struct pp_spv {
+    int N = 0, NW = 1, dev = 0, nsm = 148;
+    cudaStream_t stream = nullptr;
+    long long cap = 0;          // physical capacity of each live set
+    long long acap_phys = 0;    // physical append capacity (general path)
+    long long tcap = 0;         // sort temp capacity
+    u64 *z[2] = {nullptr, nullptr}, *x[2] = {nullptr, nullptr};
+    double *c[2] = {nullptr, nullptr};
+    int *srcidx = nullptr, *src = nullptr;
+    unsigned *meta = nullptr;
+    TileAggA *aggA = nullptr;
+    int *offA = nullptr, *hfirstA = nullptr, *fwdA = nullptr, *bwdA = nullptr;
+    int *split_i = nullptr, *split_j = nullptr;
+    u64 *tstat = nullptr, *gstat = nullptr;
+    double *part = nullptr;
+    long long nsplit_cap = 0, gtiles_cap = 0;
+    u64 *az = nullptr, *ax = nullptr, *tz = nullptr, *tx = nullptr;
+    double *ac = nullptr, *tc = nullptr;
+    int *rhist = nullptr, *rsums = nullptr;
+    long long rhist_cap = 0, rsums_cap = 0;
+    u64 *orand = nullptr;
+    double *epart = nullptr, *eout = nullptr;
+    DevState *S = nullptr;
+    DevParams *P = nullptr;
+    DevParams *Ph = nullptr;    // pinned host staging
+    GenRec *gens = nullptr;
+    long long gens_cap = 0;
+    GenRec *gens_h = nullptr;   // pinned host staging
+    long long gens_h_cap = 0;
+    int occA1 = 1, occA3 = 1, occB = 1, occG = 1;
+    long long bytes = 0;
+    long long acap_logical_init = 16;
+};
+
+// ------------------------------------------------------------------ helpers
+template <typename T>
+static int dalloc(pp_spv *h, T **p, long long count) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count <= 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, (size_t)count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(PP_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    h->bytes += (long long)count * sizeof(T);
+    return PP_OK;
+}
+
+static Bufs make_bufs(pp_spv *h) {
+    Bufs B;
+    memset(&B, 0, sizeof B);
+    for (int s = 0; s < 2; ++s) { B.z[s] = h->z[s]; B.x[s] = h->x[s]; B.c[s] = h->c[s]; }
+    B.cap = h->cap;
+    B.srcidx = h->srcidx; B.meta = h->meta; B.src = h->src;
+    B.aggA = h->aggA; B.offA = h->offA; B.hfirstA = h->hfirstA; B.fwdA = h->fwdA; B.bwdA = h->bwdA;
+    B.split_i = h->split_i; B.split_j = h->split_j; B.tstat = h->tstat; B.part = h->part;
+    B.az = h->az; B.ax = h->ax; B.ac = h->ac;
+    B.acap = h->acap_phys;
+    B.vz = h->az; B.vx = h->ax; B.vc = h->ac;
+    B.gstat = h->gstat;
+    B.S = h->S; B.P = h->P; B.gens = h->gens;
+    return B;
+}
+
+static int read_state(pp_spv *h, DevState *st) {
+    CU(cudaMemcpyAsync(st, h->S, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return PP_OK;
+}
+static int write_state(pp_spv *h, const DevState *st) {
+    CU(cudaMemcpyAsync(h->S, st, sizeof(DevState), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return PP_OK;
+}
+
+// Merge/rotate workspaces sized from the live and append capacities.
+static int alloc_merge_ws(pp_spv *h) {
+    long long need = (h->cap + std::max(h->cap, h->acap_phys)) / B_D + 4;
+    if (need > h->nsplit_cap) {
+        TRY(dalloc(h, &h->split_i, need + 1));
+        TRY(dalloc(h, &h->split_j, need + 1));
+        TRY(dalloc(h, &h->tstat, need));
+        TRY(dalloc(h, &h->part, need * 4));
+        CU(cudaMemsetAsync(h->tstat, 0, need * sizeof(u64), h->stream));
+        h->nsplit_cap = need;
+    }
+    long long g = (h->cap + h->acap_phys) / G_TILE + 4;
+    if (h->acap_phys > 0 && g > h->gtiles_cap) {
+        TRY(dalloc(h, &h->gstat, g));
+        CU(cudaMemsetAsync(h->gstat, 0, g * sizeof(u64), h->stream));
+        h->gtiles_cap = g;
+    }
+    return PP_OK;
+}
+
+// Allocates live sets and structured-path workspaces for capacity newcap,
+// preserving the live terms (copied into set 0).
+static int grow_live(pp_spv *h, long long need) {
+    long long newcap = std::max(need, std::max(2 * h->cap, (long long)4096));
+    if (newcap > 0x7fffffffll - 8192) newcap = std::max(need, 0x7fffffffll - 8192);
+    if (need > 0x7fffffffll - 8192) return fail(PP_OUT_OF_MEMORY, "term count exceeds 2^31 - 8192");
+    DevState st;
+    bool have = h->cap > 0;
+    if (have) TRY(read_state(h, &st));
+    u64 *nz = nullptr, *nx = nullptr;
+    double *nc = nullptr;
+    long long saved = h->bytes;
+    TRY(dalloc(h, &nz, newcap * h->NW));
+    TRY(dalloc(h, &nx, newcap * h->NW));
+    TRY(dalloc(h, &nc, newcap));
+    if (have && st.n > 0) {
+        CU(cudaMemcpyAsync(nz, h->z[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
+        CU(cudaMemcpyAsync(nx, h->x[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
+        CU(cudaMemcpyAsync(nc, h->c[st.cur], st.n * 8, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    CU(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < 2; ++s) {
+        if (h->z[s]) { cudaFree(h->z[s]); cudaFree(h->x[s]); cudaFree(h->c[s]); }
+        h->z[s] = nullptr; h->x[s] = nullptr; h->c[s] = nullptr;
+    }
+    h->bytes = saved - (h->cap > 0 ? 2 * h->cap * (2 * h->NW * 8 + 8) : 0);
+    h->z[0] = nz; h->x[0] = nx; h->c[0] = nc;
+    TRY(dalloc(h, &h->z[1], newcap * h->NW));
+    TRY(dalloc(h, &h->x[1], newcap * h->NW));
+    TRY(dalloc(h, &h->c[1], newcap));
+    TRY(dalloc(h, &h->srcidx, newcap));
+    TRY(dalloc(h, &h->meta, newcap));
+    TRY(dalloc(h, &h->src, newcap));
+    long long ta = newcap / A_TILE + 2;
+    TRY(dalloc(h, &h->aggA, ta));
+    TRY(dalloc(h, &h->offA, ta));
+    TRY(dalloc(h, &h->hfirstA, ta));
+    TRY(dalloc(h, &h->fwdA, ta * TAU_MAX));
+    TRY(dalloc(h, &h->bwdA, ta * TAU_MAX));
+    h->cap = newcap;
+    TRY(alloc_merge_ws(h));
+    if (have) {
+        st.cur = 0;
+        TRY(write_state(h, &st));
+    }
+    return PP_OK;
+}
+
+static int ensure_live(pp_spv *h, long long need) {
+    if (need <= h->cap) return PP_OK;
+    return grow_live(h, need);
+}
+
+// General path: physical append buffers (keeping pending appends) and sort temps.
+static int ensure_append(pp_spv *h, long long need, long long pending) {
+    if (need > h->acap_phys) {
+        long long nc = std::max(need, std::max(2 * h->acap_phys, (long long)4096));
+        u64 *nz = nullptr, *nx = nullptr;
+        double *ncc = nullptr;
+        TRY(dalloc(h, &nz, nc * h->NW));
+        TRY(dalloc(h, &nx, nc * h->NW));
+        TRY(dalloc(h, &ncc, nc));
+        if (pending > 0) {
+            CU(cudaMemcpyAsync(nz, h->az, pending * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
+            CU(cudaMemcpyAsync(nx, h->ax, pending * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
+            CU(cudaMemcpyAsync(ncc, h->ac, pending * 8, cudaMemcpyDeviceToDevice, h->stream));
+        }
+        CU(cudaStreamSynchronize(h->stream));
+        if (h->az) { cudaFree(h->az); cudaFree(h->ax); cudaFree(h->ac); }
+        h->az = nz; h->ax = nx; h->ac = ncc;
+        h->acap_phys = nc;
+        TRY(alloc_merge_ws(h));
+    }
+    if (std::max(h->acap_phys, h->cap) > h->tcap) {
+        long long tc = std::max(h->acap_phys, h->cap);
+        TRY(dalloc(h, &h->tz, tc * h->NW));
+        TRY(dalloc(h, &h->tx, tc * h->NW));
+        TRY(dalloc(h, &h->tc, tc));
+        h->tcap = tc;
+    }
+    return PP_OK;
+}
+
+static int check_err(pp_spv *h, const DevState &st) {
+    if (st.err & ERR_BOUNDS) return fail(PP_DEVICE_ERROR, "internal error: a computed index fell outside its buffer");
+    if (st.err & ERR_TIMEOUT) return fail(PP_TIMEOUT, "a device-side look-back wait timed out");
+    if (st.err & ERR_TILE) return fail(PP_ERROR_EXCEPTION, "an equal-key run exceeded the merge tile staging size");
+    return PP_OK;
+}
+
+static int sync_check(pp_spv *h) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, std::string("kernel failure: ") + cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, std::string("launch failure: ") + cudaGetErrorString(e));
+    return PP_OK;
+}
+
+// ------------------------------------------------------------------ host tables
+// lambda^k by compensated binary powering (square-and-multiply carrying each
+// product's rounding error as a double-double; x*x*x for k == 3), the
+// algorithm Julia uses for Float64^Integer.
+static double jl_pow_int(double x, long long n) {
+    if (n == 0) return 1.0;
+    double y = 1.0, xnlo = 0.0, ynlo = 0.0;
+    if (n == 3) return x * x * x;
+    if (n < 0) {
+        double rx = 1.0 / x;
+        if (n == -2) return rx * rx;
+        if (std::isfinite(x)) xnlo = -std::fma(x, rx, -1.0) * rx;
+        x = rx;
+        n = -n;
+    }
+    while (n > 1) {
+        if (n & 1) {
+            double err = std::fma(y, xnlo, x * ynlo);
+            double p = x * y;
+            ynlo = std::fma(x, y, -p);
+            y = p;
+            ynlo += err;
+        }
+        double err = x * 2.0 * xnlo;
+        double p = x * x;
+        xnlo = std::fma(x, x, -p);
+        x = p;
+        xnlo += err;
+        n >>= 1;
+    }
+    if (!std::isfinite(x)) return x * y;
+    return std::fma(x, y, std::fma(y, xnlo, x * ynlo));
+}
+
+extern "C" int pp_power_table(double lambda, int32_t kmax, double *out) {
+    if (!out || kmax < 0) return fail(PP_ARGUMENT_ERROR, "pp_power_table: bad arguments");
+    for (int k = 0; k <= kmax; ++k) out[k] = jl_pow_int(lambda, k);
+    return PP_OK;
+}
+
+static void compile_filter(const pp_filter *f, DevFilter *d) {
+    const pp_filter &F = f ? *f : NOFILTER_H;
+    d->wmax = F.wmax; d->xwmax = F.xwmax; d->mwmax = F.mwmax;
+    d->thresh = F.thresh; d->dthresh_w = F.dthresh_w; d->dthresh_xw = F.dthresh_xw;
+    d->use_mw = F.mwmax != INT64_MAX;
+    d->use_dw = F.dthresh_w >= 0.0;
+    d->use_dxw = F.dthresh_xw >= 0.0;
+    d->coeff_based = (F.thresh >= 0.0) || d->use_dw || d->use_dxw;
+    for (int w = 0; w < 130; ++w) {
+        d->expw[w] = std::exp(-F.alpha_w * (double)w);     // absc * exp(-alpha*w), spv_kernels.jl:73
+        d->expxw[w] = std::exp(-F.alpha_xw * (double)w);   // spv_kernels.jl:76
+    }
+}
+
+static bool filter_is_nofilter(const pp_filter *f) {
+    if (!f) return true;
+    return f->wmax == INT64_MAX && f->xwmax == INT64_MAX && f->mwmax == INT64_MAX && f->thresh < 0.0 &&
+           f->dthresh_w < 0.0 && f->dthresh_xw < 0.0;
+}
+
+static void load_word(const void *p, int NW, u64 *w) {
+    w[0] = w[1] = 0;
+    if (p) memcpy(w, p, NW * 8);
+}
+
+static u64 lvl_mask_all(int N, int word) {
+    int lo = 64 * word;
+    if (N <= lo) return 0;
+    if (N >= lo + 64) return ~0ull;
+    return (1ull << (N - lo)) - 1ull;
+}
+
+// Channel argument validation (channels.jl:206-207, 225-226, 236, 247, 258) and tables.
+static int build_channel(pp_spv *h, int kind, const double *prm, const void *mask, DevParams *P) {
+    if (kind < 0 || kind > 4) return fail(PP_ARGUMENT_ERROR, "unknown channel kind");
+    if (!prm) return fail(PP_ARGUMENT_ERROR, "channel parameters missing");
+    double lX, lY = 1.0, lZ = 1.0;
+    if (kind == 4) {
+        const double pX = prm[0], pY = prm[1], pZ = prm[2];
+        if (!(pX >= 0 && pY >= 0 && pZ >= 0))
+            return fail(PP_ARGUMENT_ERROR, "probabilities must be non-negative");
+        if (!(pX + pY + pZ <= 1.0 + 4.0 * 2.220446049250313e-16))
+            return fail(PP_ARGUMENT_ERROR, "pX+pY+pZ must be <= 1");
+        lX = 1.0 - 2.0 * (pY + pZ);
+        lY = 1.0 - 2.0 * (pX + pZ);
+        lZ = 1.0 - 2.0 * (pX + pY);
+    } else {
+        const double p = prm[0];
+        if (!(p >= 0.0 && p <= 1.0)) return fail(PP_ARGUMENT_ERROR, "channel parameter p must be in [0,1]");
+        lX = kind == 0 ? 1.0 - 4.0 * p / 3.0 : 1.0 - 2.0 * p;
+    }
+    P->chan_kind = kind;
+    for (int k = 0; k < 130; ++k) {
+        P->chanX[k] = jl_pow_int(lX, k);
+        P->chanY[k] = jl_pow_int(lY, k);
+        P->chanZ[k] = jl_pow_int(lZ, k);
+    }
+    if (mask) {
+        load_word(mask, h->NW, P->chan_mask);
+    } else {
+        P->chan_mask[0] = lvl_mask_all(h->N, 0);
+        P->chan_mask[1] = h->NW == 2 ? lvl_mask_all(h->N, 1) : 0;
+    }
+    return PP_OK;
+}
+
+static int upload_params(pp_spv *h) {
+    CU(cudaMemcpyAsync(h->P, h->Ph, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return PP_OK;
+}
+
+// GenRec for one generator: mask levels (descending) of M = (gz, gx).
+static int make_gen(const pp_spv *h, const u64 *gz, const u64 *gx, double cv, double sv, GenRec *g, bool *structured) {
+    memset(g, 0, sizeof *g);
+    for (int w = 0; w < 2; ++w) { g->gz[w] = w < h->NW ? gz[w] : 0; g->gx[w] = w < h->NW ? gx[w] : 0; }
+    g->cosv = cv;
+    g->sinv = sv;
+    int ng = 0;
+    for (int w = 0; w < h->NW; ++w) ng += __builtin_popcountll(g->gz[w] & g->gx[w]);
+    g->ng = ng;
+    int k = 0;
+    bool ok = true;
+    for (int lvl = 128 * h->NW - 1; lvl >= 0; --lvl) {
+        int bit;
+        if (lvl >= 64 * h->NW) { int l = lvl - 64 * h->NW; bit = (int)((g->gz[l >> 6] >> (l & 63)) & 1); }
+        else bit = (int)((g->gx[lvl >> 6] >> (lvl & 63)) & 1);
+        if (!bit) continue;
+        if (k < KMAX) g->level[k] = (short)lvl;
+        ++k;
+    }
+    if (k > KMAX) { ok = false; k = KMAX; }
+    g->k = k;
+    *structured = ok;
+    return PP_OK;
+}
+
+// ------------------------------------------------------------------ launches
+template <int NW>
+static int launch_setup(pp_spv *h) {
+    CU(cudaFuncSetAttribute(k_classify<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(2 * NW * A_TILE * 8 + A_TILE)));
+    CU(cudaFuncSetAttribute(k_merge<NW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    CU(cudaFuncSetAttribute(k_merge<NW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    CU(cudaFuncSetAttribute(k_merge<NW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    int occ = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_classify<NW>, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE));
+    h->occA1 = std::max(1, occ);
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_permute<NW>, A_THREADS, 0));
+    h->occA3 = std::max(1, occ);
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_merge<NW, 0>, B_THREADS, merge_smem_bytes<NW>()));
+    h->occB = std::max(1, occ);
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rotate_general<NW>, G_THREADS, 0));
+    h->occG = std::max(1, occ);
+    return PP_OK;
+}
+
+// One structured window-1 rotation: 6 launches, no host synchronisation.
+template <int NW>
+static void launch_struct_rotation(pp_spv *h, const Bufs &B) {
+    cudaStream_t s = h->stream;
+    k_classify<NW><<<h->nsm * h->occA1, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE, s>>>(B);
+    k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
+    k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
+    k_partition<NW, 0><<<h->nsm * 4, 256, 0, s>>>(B);
+    k_merge<NW, 0><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, 0);
+    k_commit<0><<<1, 256, 0, s>>>(B, 0);
+}
+
+template <int NW, int MODE>
+static void launch_merge(pp_spv *h, const Bufs &B, int flags) {
+    cudaStream_t s = h->stream;
+    k_partition<NW, MODE><<<h->nsm * 4, 256, 0, s>>>(B);
+    k_merge<NW, MODE><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, flags);
+    k_commit<MODE><<<1, 256, 0, s>>>(B, flags);
+}
+
+// Stable LSD radix sort of n records in set A (za, xa, ca) using set T as the
+// ping-pong partner.  *in_t = 1 if the result ended in T.
+template <int NW>
+static int radix_sort(pp_spv *h, u64 *za, u64 *xa, double *ca, u64 *zt, u64 *xt, double *ct, long long n, int *in_t) {
+    *in_t = 0;
+    if (n <= 1) return PP_OK;
+    cudaStream_t s = h->stream;
+    u64 init[8] = {0, 0, 0, 0, ~0ull, ~0ull, ~0ull, ~0ull};
+    CU(cudaMemcpyAsync(h->orand, init, sizeof init, cudaMemcpyHostToDevice, s));
+    k_keybits<NW><<<h->nsm * 4, 256, 0, s>>>(za, xa, n, h->orand);
+    u64 orand[8];
+    CU(cudaMemcpyAsync(orand, h->orand, sizeof orand, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const int ntiles = (int)((n + R_TILE - 1) / R_TILE);
+    const long long m = 256ll * ntiles;
+    if (m > h->rhist_cap) { TRY(dalloc(h, &h->rhist, m)); h->rhist_cap = m; }
+    const long long nb = (m + SC_TILE - 1) / SC_TILE;
+    if (nb > h->rsums_cap) { TRY(dalloc(h, &h->rsums, nb)); h->rsums_cap = nb; }
+    u64 *cz = za, *cx = xa, *oz = zt, *ox = xt;
+    double *cc = ca, *oc = ct;
+    int passes = 0;
+    for (int d = 0; d < 16 * NW; ++d) {
+        const int lvl = 8 * d;
+        u64 vary;
+        if (lvl >= 64 * NW) { int l = lvl - 64 * NW; vary = (orand[l >> 6] ^ orand[4 + (l >> 6)]) >> (l & 63); }
+        else vary = (orand[NW + (lvl >> 6)] ^ orand[4 + NW + (lvl >> 6)]) >> (lvl & 63);
+        if ((vary & 0xffull) == 0) continue;
+        const int grid = std::min(ntiles, h->nsm * 8);
+        k_radix_hist<NW><<<grid, R_THREADS, 0, s>>>(cz, cx, n, d, h->rhist, ntiles);
+        k_scan_tiles<<<(int)nb, SC_THREADS, 0, s>>>(h->rhist, m, h->rsums);
+        k_scan_sums<<<1, 1024, 0, s>>>(h->rsums, (int)nb);
+        k_scan_add<<<(int)((m + 255) / 256), 256, 0, s>>>(h->rhist, m, h->rsums);
+        k_radix_scatter<NW><<<grid, R_THREADS, 0, s>>>(cz, cx, cc, n, d, h->rhist, ntiles, oz, ox, oc);
+        std::swap(cz, oz); std::swap(cx, ox); std::swap(cc, oc);
+        ++passes;
+    }
+    *in_t = passes & 1;
+    return sync_check(h);
+}
+
+static int radix_sort_nw(pp_spv *h, u64 *za, u64 *xa, double *ca, u64 *zt, u64 *xt, double *ct, long long n, int *in_t) {
+    return h->NW == 1 ? radix_sort<1>(h, za, xa, ca, zt, xt, ct, n, in_t)
+                      : radix_sort<2>(h, za, xa, ca, zt, xt, ct, n, in_t);
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" int pp_create(int32_t N, int64_t live_cap, int64_t append_cap, pp_spv **out) {
+    if (!out) return fail(PP_ARGUMENT_ERROR, "pp_create: out is NULL");
+    *out = nullptr;
+    if (N < 0) return fail(PP_ARGUMENT_ERROR, "N must be >= 0");
+    if (N > 128) return fail(PP_ERROR_EXCEPTION, "N > 128 requires a multi-word type (add BitIntegers.jl and extend _word_type)");
+    pp_spv *h = new pp_spv();
+    h->N = N;
+    h->NW = N <= 64 ? 1 : 2;
+    h->acap_logical_init = std::max<int64_t>(1, append_cap);
+    auto bail = [&](int code) { pp_destroy(h); return code; };
+    cudaError_t e = cudaGetDevice(&h->dev);
+    if (e != cudaSuccess) { g_err = std::string("no CUDA device: ") + cudaGetErrorString(e); delete h; return PP_DEVICE_ERROR; }
+    cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->dev);
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { g_err = cudaGetErrorString(e); delete h; return PP_DEVICE_ERROR; }
+    int r = h->NW == 1 ? launch_setup<1>(h) : launch_setup<2>(h);
+    if (r) return bail(r);
+    if ((r = dalloc(h, &h->S, 1))) return bail(r);
+    if ((r = dalloc(h, &h->P, 1))) return bail(r);
+    if ((r = dalloc(h, &h->orand, 8))) return bail(r);
+    if ((r = dalloc(h, &h->epart, 4096))) return bail(r);
+    if ((r = dalloc(h, &h->eout, 1))) return bail(r);
+    if (cudaMallocHost((void **)&h->Ph, sizeof(DevParams)) != cudaSuccess) return bail(fail(PP_OUT_OF_MEMORY, "cudaMallocHost"));
+    memset(h->Ph, 0, sizeof(DevParams));
+    h->Ph->chan_kind = -1;
+    compile_filter(nullptr, &h->Ph->strict);
+    compile_filter(nullptr, &h->Ph->local);
+    compile_filter(nullptr, &h->Ph->clip);
+    if ((r = upload_params(h))) return bail(r);
+    DevState st;
+    memset(&st, 0, sizeof st);
+    st.acap_logical = h->acap_logical_init;
+    if ((r = write_state(h, &st))) return bail(r);
+    if ((r = grow_live(h, std::max<int64_t>(live_cap, 4096)))) return bail(r);
+    *out = h;
+    return PP_OK;
+}
+
+extern "C" int pp_destroy(pp_spv *h) {
+    if (!h) return PP_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void *ptrs[] = {h->z[0], h->z[1], h->x[0], h->x[1], h->c[0], h->c[1], h->srcidx, h->src, h->meta, h->aggA,
+                    h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
+                    h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
+                    h->S, h->P, h->gens};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    if (h->Ph) cudaFreeHost(h->Ph);
+    if (h->gens_h) cudaFreeHost(h->gens_h);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return PP_OK;
+}
+
+extern "C" int pp_upload(pp_spv *h, const void *z, const void *x, const double *c, int64_t n, int32_t sorted) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    if (n < 0) return fail(PP_ARGUMENT_ERROR, "n must be >= 0");
+    if (n > 0 && (!z || !x || !c)) return fail(PP_ARGUMENT_ERROR, "null term arrays");
+    DevState st;
+    TRY(read_state(h, &st));
+    st.n = 0; st.an = 0; st.cur = 0; st.err = 0;
+    TRY(write_state(h, &st));
+    TRY(ensure_live(h, n));
+    const size_t wb = (size_t)h->NW * 8;
+    if (n > 0) {
+        CU(cudaMemcpyAsync(h->z[0], z, n * wb, cudaMemcpyDefault, h->stream));
+        CU(cudaMemcpyAsync(h->x[0], x, n * wb, cudaMemcpyDefault, h->stream));
+        CU(cudaMemcpyAsync(h->c[0], c, n * 8, cudaMemcpyDefault, h->stream));
+    }
+    TRY(read_state(h, &st));
+    st.n = n; st.cur = 0;
+    if (!sorted && n > 1) {
+        int in_t = 0;
+        TRY(radix_sort_nw(h, h->z[0], h->x[0], h->c[0], h->z[1], h->x[1], h->c[1], n, &in_t));
+        st.cur = in_t;
+    }
+    TRY(write_state(h, &st));
+    return PP_OK;
+}
+
+extern "C" int pp_download(pp_spv *h, void *z, void *x, double *c, int64_t cap, int64_t *n) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long m = std::min<long long>(st.n, std::max<int64_t>(cap, 0));
+    const size_t wb = (size_t)h->NW * 8;
+    if (m > 0) {
+        if (z) CU(cudaMemcpyAsync(z, h->z[st.cur], m * wb, cudaMemcpyDefault, h->stream));
+        if (x) CU(cudaMemcpyAsync(x, h->x[st.cur], m * wb, cudaMemcpyDefault, h->stream));
+        if (c) CU(cudaMemcpyAsync(c, h->c[st.cur], m * 8, cudaMemcpyDefault, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    if (n) *n = st.n;
+    return PP_OK;
+}
+
+extern "C" int pp_length(pp_spv *h, int64_t *n) {
+    if (!h || !n) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState st;
+    TRY(read_state(h, &st));
+    *n = st.n;
+    return PP_OK;
+}
+
+extern "C" int pp_copy(pp_spv *h, pp_spv **out) {
+    if (!h || !out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState st;
+    TRY(read_state(h, &st));
+    pp_spv *o = nullptr;
+    TRY(pp_create(h->N, st.n, st.acap_logical, &o));
+    const size_t wb = (size_t)h->NW * 8;
+    if (st.n > 0) {
+        cudaMemcpyAsync(o->z[0], h->z[st.cur], st.n * wb, cudaMemcpyDeviceToDevice, o->stream);
+        cudaMemcpyAsync(o->x[0], h->x[st.cur], st.n * wb, cudaMemcpyDeviceToDevice, o->stream);
+        cudaMemcpyAsync(o->c[0], h->c[st.cur], st.n * 8, cudaMemcpyDeviceToDevice, o->stream);
+    }
+    DevState so;
+    memset(&so, 0, sizeof so);
+    so.n = st.n;
+    so.acap_logical = st.acap_logical;
+    int r = write_state(o, &so);
+    if (r) { pp_destroy(o); return r; }
+    *out = o;
+    return PP_OK;
+}
+
+static int ensure_gens(pp_spv *h, long long L) {
+    if (L > h->gens_cap) {
+        TRY(dalloc(h, &h->gens, L));
+        h->gens_cap = L;
+    }
+    if (L > h->gens_h_cap) {
+        if (h->gens_h) cudaFreeHost(h->gens_h);
+        if (cudaMallocHost((void **)&h->gens_h, L * sizeof(GenRec)) != cudaSuccess)
+            return fail(PP_OUT_OF_MEMORY, "cudaMallocHost");
+        h->gens_h_cap = L;
+    }
+    return PP_OK;
+}
+
+// Per-call accounting of launches and (when profiling) per-kernel device time.
+struct RunProf {
+    bool on = false;
+    double t_rotate = 0, t_partition = 0, t_merge = 0;
+    long long launches = 0;
+};
+
+// Structured window-1 sequence: chunks of CHUNK_ROT rotations between state
+// read-backs; on ERR_OVERFLOW grow and resume at the rotation that stopped.
+template <int NW>
+static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
+    long long done = 0;
+    const bool timed = prof->on || (ctr && (ctr->t_rotate || ctr->t_merge));
+    std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
+    while (done < L) {
+        Bufs B = make_bufs(h);
+        const long long end = std::min(L, done + CHUNK_ROT);
+        cudaStream_t s = h->stream;
+        for (long long r = done; r < end; ++r) {
+            if (!timed) {
+                launch_struct_rotation<NW>(h, B);
+            } else {
+                cudaEvent_t e[5];
+                for (int q = 0; q < 5; ++q) cudaEventCreate(&e[q]);
+                cudaEventRecord(e[0], s);
+                k_classify<NW><<<h->nsm * h->occA1, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE, s>>>(B);
+                k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
+                k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
+                cudaEventRecord(e[1], s);
+                k_partition<NW, 0><<<h->nsm * 4, 256, 0, s>>>(B);
+                cudaEventRecord(e[2], s);
+                k_merge<NW, 0><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, 0);
+                cudaEventRecord(e[3], s);
+                k_commit<0><<<1, 256, 0, s>>>(B, 0);
+                cudaEventRecord(e[4], s);
+                for (int q = 0; q < 5; ++q) ev.push_back(e[q]);
+            }
+            prof->launches += 6;
+        }
+        TRY(sync_check(h));
+        DevState st;
+        TRY(read_state(h, &st));
+        if (timed) {
+            // rotations that ran are [done, st.rot); the rest were no-ops
+            const long long base = (long long)ev.size() / 5 - (end - done);
+            for (long long r = done; r < end; ++r) {
+                cudaEvent_t *e = &ev[(base + (r - done)) * 5];
+                if (r < st.rot) {
+                    float a = 0, b = 0, c = 0, d = 0;
+                    cudaEventElapsedTime(&a, e[0], e[1]);
+                    cudaEventElapsedTime(&b, e[1], e[2]);
+                    cudaEventElapsedTime(&c, e[2], e[3]);
+                    cudaEventElapsedTime(&d, e[3], e[4]);
+                    prof->t_rotate += a * 1e-3;
+                    prof->t_partition += (b + d) * 1e-3;
+                    prof->t_merge += c * 1e-3;
+                    if (ctr && r < ctr->nwin) {
+                        if (ctr->t_rotate) ctr->t_rotate[r] += a * 1e-3;
+                        if (ctr->t_merge) ctr->t_merge[r] += (b + c + d) * 1e-3;
+                    }
+                }
+                for (int q = 0; q < 5; ++q) cudaEventDestroy(e[q]);
+            }
+            ev.clear();
+        }
+        if (st.err & ERR_OVERFLOW) {
+            st.err &= ~ERR_OVERFLOW;
+            TRY(write_state(h, &st));
+            TRY(ensure_live(h, std::max(st.need + st.need / 2, 2 * st.n)));
+            done = st.rot;
+            continue;
+        }
+        TRY(check_err(h, st));
+        done = st.rot;
+        // grow ahead of time when the live set approaches capacity
+        if (done < L && 2 * st.n > h->cap) TRY(ensure_live(h, 4 * st.n));
+    }
+    return PP_OK;
+}
+
+// General path boundary: sort pending appends, merge (MODE 1).
+template <int NW>
+static int general_boundary(pp_spv *h, int flags, long long *n_in, long long *n_out) {
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long an = st.an;
+    *n_in = st.n + an;
+    TRY(ensure_live(h, st.n + an));
+    TRY(read_state(h, &st));
+    Bufs B = make_bufs(h);
+    if (an > 0) {
+        int in_t = 0;
+        TRY(ensure_append(h, h->acap_phys, an));
+        TRY(radix_sort<NW>(h, h->az, h->ax, h->ac, h->tz, h->tx, h->tc, an, &in_t));
+        B = make_bufs(h);
+        if (in_t) { B.vz = h->tz; B.vx = h->tx; B.vc = h->tc; }
+    }
+    launch_merge<NW, 1>(h, B, flags);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    TRY(check_err(h, st));
+    *n_out = st.n;
+    return PP_OK;
+}
+
+// General path: the sequence driver of spv_evolve.jl:352-385 with host decisions.
+// `period` > 0 makes every period-th rotation end a separate evolve! call (the
+// window count restarts and a boundary closes the layer), which is the
+// semantics of a loop "evolve!(v, layer; ...); channel!(v, p)".
+template <int NW>
+static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window, pp_counters *ctr, int last_flags,
+                       long long period, int chan_flags, RunProf *prof) {
+    const long long L = (long long)G.size();
+    long long since = 0;
+    for (long long i = 1; i <= L; ++i) {
+        const long long w = (i + window - 1) / window;
+        const long long irel = period > 0 ? (i - 1) % period + 1 : i;
+        DevState st;
+        TRY(read_state(h, &st));
+        if (2 * st.an + st.n > st.acap_logical) {
+            long long ni, no;
+            TRY(general_boundary<NW>(h, 0, &ni, &no));
+            since = 0;
+            TRY(read_state(h, &st));
+            if (ctr && w <= ctr->nwin) {
+                if (ctr->early_merges) ctr->early_merges[w - 1] += 1;
+                if (ctr->merge_in) ctr->merge_in[w - 1] += ni;
+                if (ctr->merge_out) ctr->merge_out[w - 1] += no;
+            }
+            if (st.n > st.acap_logical) {
+                st.acap_logical = std::max(2 * st.acap_logical, st.n);
+                TRY(write_state(h, &st));
+            }
+        }
+        TRY(ensure_append(h, std::max(st.acap_logical, 2 * st.an + st.n), st.an));
+        TRY(alloc_merge_ws(h));
+        Bufs B = make_bufs(h);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (ctr && ctr->t_rotate) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, h->stream); }
+        const long long an_before = st.an;
+        const int ntiles = (int)std::max(1ll, (st.n + st.an + G_TILE - 1) / G_TILE);
+        k_rotate_general<NW><<<std::min(ntiles, h->nsm * h->occG), G_THREADS, 0, h->stream>>>(B, G[i - 1]);
+        k_rotate_commit<<<1, 1, 0, h->stream>>>(B);
+        if (e1) cudaEventRecord(e1, h->stream);
+        TRY(sync_check(h));
+        TRY(read_state(h, &st));
+        TRY(check_err(h, st));
+        if (ctr && w <= ctr->nwin) {
+            if (ctr->terms_created) ctr->terms_created[w - 1] += st.an - an_before;
+            if (e0) { float ms = 0; cudaEventElapsedTime(&ms, e0, e1); ctr->t_rotate[w - 1] += ms * 1e-3; }
+        }
+        if (e0) { cudaEventDestroy(e0); cudaEventDestroy(e1); }
+        since++;
+        prof->launches += 2;
+        const bool layer_end = period > 0 && irel == period;
+        if (irel % window == 0 || layer_end || i == L) {
+            long long ni, no;
+            cudaEvent_t m0 = nullptr, m1 = nullptr;
+            if (ctr && ctr->t_merge) { cudaEventCreate(&m0); cudaEventCreate(&m1); cudaEventRecord(m0, h->stream); }
+            const int fl = (i == L ? last_flags : 0) | (layer_end ? chan_flags : 0);
+            TRY(general_boundary<NW>(h, fl, &ni, &no));
+            prof->launches += 3;
+            if (m0) {
+                cudaEventRecord(m1, h->stream);
+                cudaEventSynchronize(m1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, m0, m1);
+                if (w <= ctr->nwin) ctr->t_merge[w - 1] += ms * 1e-3;
+                cudaEventDestroy(m0); cudaEventDestroy(m1);
+            }
+            if (ctr && w <= ctr->nwin) {
+                if (ctr->merge_in) ctr->merge_in[w - 1] += ni;
+                if (ctr->merge_out) ctr->merge_out[w - 1] += no;
+            }
+            since = 0;
+        }
+    }
+    return PP_OK;
+}
+
+static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *cosv, const double *sinv, int64_t L,
+                       const pp_evolve_opts *o) {
+    pp_evolve_opts def;
+    memset(&def, 0, sizeof def);
+    def.window = 1;
+    def.chan_kind = -1;
+    const pp_evolve_opts &O = o ? *o : def;
+    if (O.window < 1) return fail(PP_ARGUMENT_ERROR, "window must be >= 1");
+    if (L < 0) return fail(PP_DIMENSION_MISMATCH, "generators and angles must have same length");
+    if (L > 0 && (!gz || !gx || !cosv || !sinv)) return fail(PP_ARGUMENT_ERROR, "null generator arrays");
+    if (O.strict_kind != 0) return fail(PP_NOT_IMPLEMENTED, "AdaptiveTruncation has no GPU merge path yet (no CPU fallback)");
+    if (O.corr_kind != 0 && O.corr_kind != 1)
+        return fail(PP_NOT_IMPLEMENTED, "only NoCorrection and EnergyCorrection run on the GPU");
+    // parameters
+    DevParams *P = h->Ph;
+    compile_filter(O.strict, &P->strict);
+    compile_filter(O.local, &P->local);
+    P->local_active = filter_is_nofilter(O.local) ? 0 : 1;
+    P->corr_kind = O.corr_kind;
+    load_word(O.ket, h->NW, P->ket);
+    P->chan_kind = -1;
+    if (O.chan_kind >= 0) TRY(build_channel(h, O.chan_kind, O.chan_prm, O.chan_mask, P));
+    if (L == 0) {
+        if (O.chan_kind >= 0) {
+            TRY(upload_params(h));
+            Bufs B = make_bufs(h);
+            if (h->NW == 1) k_channel<1><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+            else k_channel<2><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+            TRY(sync_check(h));
+        }
+        return PP_OK;
+    }
+    TRY(upload_params(h));
+    // generators
+    TRY(ensure_gens(h, L));
+    std::vector<GenRec> G((size_t)L);
+    bool all_struct = true;
+    const size_t wb = (size_t)h->NW * 8;
+    for (long long i = 0; i < L; ++i) {
+        u64 wz[2] = {0, 0}, wx[2] = {0, 0};
+        memcpy(wz, (const char *)gz + i * wb, wb);
+        memcpy(wx, (const char *)gx + i * wb, wb);
+        bool st = true;
+        make_gen(h, wz, wx, cosv[i], sinv[i], &G[i], &st);
+        all_struct = all_struct && st;
+    }
+    const bool chan = O.chan_kind >= 0;
+    const long long period = (chan && O.chan_every > 0) ? O.chan_every : 0;
+    const int last_flags = GEN_MEASURE | ((chan && period == 0) ? GEN_CHANNEL : 0);
+    G[L - 1].flags |= last_flags;
+    if (period > 0)
+        for (long long i = period - 1; i < L; i += period) G[i].flags |= GEN_CHANNEL;
+    memcpy(h->gens_h, G.data(), L * sizeof(GenRec));
+    CU(cudaMemcpyAsync(h->gens, h->gens_h, L * sizeof(GenRec), cudaMemcpyHostToDevice, h->stream));
+    // state for this call
+    DevState st;
+    TRY(read_state(h, &st));
+    st.rot = 0; st.rot_end = L;
+    st.created = st.merge_in = st.merge_out = st.early = 0;
+    st.npref = 0;
+    st.live_in = 0;
+    st.peak = 0;
+    st.corr_energy = O.corr_energy ? *O.corr_energy : 0.0;
+    st.measure_valid = 0;
+    st.b_tile_ctr = 0; st.g_tile_ctr = 0;
+    TRY(write_state(h, &st));
+    pp_counters *ctr = O.counters;
+    RunProf prof;
+    prof.on = O.profile != 0;
+    if (O.window == 1 && all_struct) {
+        TRY(ensure_live(h, 2 * st.n + 16));
+        if (h->NW == 1) TRY(run_struct<1>(h, L, ctr, &prof));
+        else TRY(run_struct<2>(h, L, ctr, &prof));
+    } else {
+        if (h->NW == 1) TRY(run_general<1>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
+        else TRY(run_general<2>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
+    }
+    TRY(read_state(h, &st));
+    TRY(check_err(h, st));
+    if (O.corr_energy) *O.corr_energy = st.corr_energy;
+    if (O.expect_out) *O.expect_out = st.expect_val;
+    if (O.stats_out) {
+        double *so = O.stats_out;
+        for (int i = 0; i < PP_STATS_LEN; ++i) so[i] = 0.0;
+        so[PP_STAT_TERMS_IN] = (double)st.live_in;
+        so[PP_STAT_CREATED] = (double)st.created;
+        so[PP_STAT_MERGE_IN] = (double)st.merge_in;
+        so[PP_STAT_MERGE_OUT] = (double)st.merge_out;
+        so[PP_STAT_PEAK] = (double)st.peak;
+        so[PP_STAT_EARLY] = (double)st.early;
+        so[PP_STAT_T_ROTATE] = prof.t_rotate;
+        so[PP_STAT_T_MERGE] = prof.t_merge;
+        so[PP_STAT_LAUNCHES] = (double)prof.launches;
+        so[PP_STAT_T_PARTITION] = prof.t_partition;
+    }
+    return PP_OK;
+}
+
+extern "C" int pp_evolve(pp_spv *h, const void *gz, const void *gx, const double *cosv, const double *sinv, int64_t L,
+                         const pp_evolve_opts *opts) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    return evolve_impl(h, gz, gx, cosv, sinv, L, opts);
+}
+
+extern "C" int pp_evolve1(pp_spv *h, const void *gz, const void *gx, double cos_theta, double sin_theta) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    // evolve!(O, G, θ): grow the append capacity to n + 2an first (spv_evolve.jl:231),
+    // which is what the early-merge rule of later sequence calls sees.
+    DevState st;
+    TRY(read_state(h, &st));
+    if (st.n + 2 * st.an > st.acap_logical) {
+        st.acap_logical = std::max(2 * st.acap_logical, st.n + 2 * st.an);
+        TRY(write_state(h, &st));
+    }
+    pp_evolve_opts o;
+    memset(&o, 0, sizeof o);
+    o.window = 1;
+    o.chan_kind = -1;
+    return evolve_impl(h, gz, gx, &cos_theta, &sin_theta, 1, &o);
+}
+
+extern "C" int pp_compact(pp_spv *h, const pp_filter *f) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    compile_filter(f, &h->Ph->clip);
+    TRY(upload_params(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    st.an = 0;
+    TRY(write_state(h, &st));
+    Bufs B = make_bufs(h);
+    if (h->NW == 1) launch_merge<1, 2>(h, B, 0);
+    else launch_merge<2, 2>(h, B, 0);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    return check_err(h, st);
+}
+
+extern "C" int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh) {
+    (void)max_terms; (void)min_thresh;
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    return fail(PP_NOT_IMPLEMENTED, "AdaptiveTruncation has no GPU path yet (no CPU fallback)");
+}
+
+extern "C" int pp_channel(pp_spv *h, int32_t kind, const double *prm, const void *qubit_mask) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    TRY(build_channel(h, kind, prm, qubit_mask, h->Ph));
+    TRY(upload_params(h));
+    Bufs B = make_bufs(h);
+    if (h->NW == 1) k_channel<1><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+    else k_channel<2><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+    return sync_check(h);
+}
+
+extern "C" int pp_expect_ket(pp_spv *h, const void *ket, double *out) {
+    if (!h || !out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    u64 k[2];
+    load_word(ket, h->NW, k);
+    Bufs B = make_bufs(h);
+    const int nb = std::min(4096, h->nsm * 8);
+    if (h->NW == 1) k_expect<1><<<nb, 256, 0, h->stream>>>(B, k[0], k[1], h->epart);
+    else k_expect<2><<<nb, 256, 0, h->stream>>>(B, k[0], k[1], h->epart);
+    k_expect_final<<<1, 32, 0, h->stream>>>(h->epart, nb, h->eout);
+    CU(cudaMemcpyAsync(out, h->eout, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return sync_check(h);
+}
+
+extern "C" int pp_check(pp_spv *h, int32_t *ok) {
+    if (!h || !ok) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState st;
+    TRY(read_state(h, &st));
+    st.err &= ~ERR_CHECK;
+    TRY(write_state(h, &st));
+    Bufs B = make_bufs(h);
+    if (h->NW == 1) k_check<1><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+    else k_check<2><<<h->nsm * 8, 256, 0, h->stream>>>(B);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    *ok = (!(st.err & ERR_CHECK) && st.n <= h->cap && st.an == 0) ? 1 : 0;
+    st.err &= ~ERR_CHECK;
+    TRY(write_state(h, &st));
+    return PP_OK;
+}
+
+extern "C" int pp_stream(pp_spv *h, void **stream) {
+    if (!h || !stream) return fail(PP_ARGUMENT_ERROR, "null argument");
+    *stream = (void *)h->stream;
+    return PP_OK;
+}
+
+extern "C" int pp_device_bytes(pp_spv *h, int64_t *bytes) {
+    if (!h || !bytes) return fail(PP_ARGUMENT_ERROR, "null argument");
+    *bytes = h->bytes;
+    return PP_OK;
+}

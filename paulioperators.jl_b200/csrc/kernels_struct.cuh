@@ -1,0 +1,707 @@
+// Window-1 rotation as one sort-free pass structure (the GPU counterpart of
+// _rotate_range! + _gather_append! + _unshuffle_ws! + _try_merge!,
+// spv_kernels.jl:146-177, 187-193, 262-363, driven as in spv_evolve.jl:352-385).
+//
+// The sin branches of one rotation are the keys P xor M (M = (gz, gx)) of the
+// anticommuting live terms P.  Since live is sorted, the appended keys are
+// sorted by key xor M; their sorted position is the classic rank identity
+//   rank(P xor M) = rank(P) + sum_{b in M} ([P_b = 0] - [P_b = 1]) * sib_b(P),
+// where sib_b(P) counts emitted terms that share P's bits above level b and
+// differ at b.  sib_b comes from the positions where the "highest differing
+// bit" h between consecutive emitted keys crosses b and b+1, i.e. from
+// forward/backward max/min scans.  Kernels:
+//   k_classify  (A1) tile-local compaction of emitting terms, h, tile aggregates
+//   k_tilescan  (A2) one CTA: tile offsets and cross-tile scan carries
+//   k_permute   (A3) final ranks -> src[rank] = live index (no key traffic)
+//   k_partition (P)  merge-path split of (live, virtual sorted appends)
+//   k_merge     (B)  merge + reduce-by-key + filter + channel + compaction
+// The appended keys are never materialised: B gathers live[src[k]] and applies
+// the xor and the phase on the fly.
+#pragma once
+#include "blockscan.cuh"
+
+namespace pp {
+
+struct Bufs {
+    u64 *z[2], *x[2];
+    double *c[2];
+    long long cap;
+    // structured path
+    int *srcidx;
+    unsigned *meta;
+    int *src;
+    TileAggA *aggA;
+    int *offA, *hfirstA, *fwdA, *bwdA;
+    // merge
+    int *split_i, *split_j;
+    u64 *tstat;
+    double *part;
+    // general path (direct V = sorted appends)
+    u64 *az, *ax;
+    double *ac;
+    long long acap;
+    u64 *vz, *vx;
+    double *vc;
+    u64 *gstat;
+    DevState *S;
+    const DevParams *P;
+    const GenRec *gens;
+};
+
+__device__ __forceinline__ int tau_value(const GenRec &g, int tau) {
+    return (int)g.level[tau >> 1] + (tau & 1);
+}
+
+// ---------------------------------------------------------------- A1 classify
+template <int NW>
+__global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
+    DevState *S = B.S;
+    if (S->err) return;
+    const long long rot = S->rot;
+    if (rot >= S->rot_end) return;
+    __shared__ GenRec g;
+    __shared__ int wtot[A_ITEMS * (A_THREADS / 32)];
+    __shared__ int s_total;
+    __shared__ int s_first[TAU_MAX], s_last[TAU_MAX];
+    extern __shared__ u64 sm[];
+    u64 *skz = sm;                    // [NW][A_TILE]
+    u64 *skx = sm + NW * A_TILE;      // [NW][A_TILE]
+    unsigned char *sh = reinterpret_cast<unsigned char *>(sm + 2 * NW * A_TILE);  // [A_TILE]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) g = B.gens[rot];
+    __syncthreads();
+    const DevParams &P = *B.P;
+    const long long n = S->n;
+    const int cur = S->cur;
+    const bool pref = n > S->acap_logical;
+    const bool local_on = P.local_active != 0;
+    const u64 *Z = B.z[cur], *X = B.x[cur];
+    const double *C = B.c[cur];
+    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    const int ntau = 2 * g.k;
+
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long base = (long long)t * A_TILE;
+        const int tcnt = (int)min((long long)A_TILE, n - base);
+        bool emit[A_ITEMS];
+        Key<NW> key[A_ITEMS];
+#pragma unroll
+        for (int it = 0; it < A_ITEMS; ++it) {
+            const int idx = it * A_THREADS + tid;
+            emit[it] = false;
+            if (idx < tcnt) {
+                key[it] = load_key<NW>(Z, X, base + idx);
+                Key<NW> q;
+                double sg;
+                if (rotate_term<NW>(key[it], g, &q, &sg)) {
+                    bool ok = true;
+                    if (pref || local_on) {
+                        const double c = C[base + idx];
+                        if (pref && should_drop<NW>(P.strict, key[it], fabs(c))) ok = false;
+                        if (ok && local_on) {
+                            const double cn = __dmul_rn(sg * g.sinv, c);
+                            if (should_drop<NW>(P.local, q, fabs(cn))) ok = false;
+                        }
+                    }
+                    emit[it] = ok;
+                }
+            }
+        }
+        int lpre[A_ITEMS];
+#pragma unroll
+        for (int it = 0; it < A_ITEMS; ++it) {
+            unsigned m = __ballot_sync(0xffffffffu, emit[it]);
+            lpre[it] = __popc(m & lanemask_lt());
+            if (lane == 0) wtot[it * (A_THREADS / 32) + warp] = __popc(m);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            constexpr int NE = A_ITEMS * (A_THREADS / 32);  // 128 entries, 4 per lane
+            int v[NE / 32];
+            int s = 0;
+#pragma unroll
+            for (int q = 0; q < NE / 32; ++q) { v[q] = wtot[lane * (NE / 32) + q]; s += v[q]; }
+            int incl = warp_incl_scan(s, OpSum());
+            int ex = incl - s;
+#pragma unroll
+            for (int q = 0; q < NE / 32; ++q) { wtot[lane * (NE / 32) + q] = ex; ex += v[q]; }
+            if (lane == 31) s_total = incl;
+        }
+        if (tid < TAU_MAX) { s_first[tid] = 0x7fff; s_last[tid] = -1; }
+        __syncthreads();
+        const int total = s_total;
+#pragma unroll
+        for (int it = 0; it < A_ITEMS; ++it) {
+            if (emit[it]) {
+                const int j = wtot[it * (A_THREADS / 32) + warp] + lpre[it];
+#pragma unroll
+                for (int w = 0; w < NW; ++w) { skz[w * A_TILE + j] = key[it].z[w]; skx[w * A_TILE + j] = key[it].x[w]; }
+                B.srcidx[base + j] = (int)(base + it * A_THREADS + tid);
+            }
+        }
+        __syncthreads();
+        for (int j = tid; j < total; j += A_THREADS) {
+            Key<NW> kj;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) { kj.z[w] = skz[w * A_TILE + j]; kj.x[w] = skx[w * A_TILE + j]; }
+            int h = 0xff;
+            if (j > 0) {
+                Key<NW> kp;
+#pragma unroll
+                for (int w = 0; w < NW; ++w) { kp.z[w] = skz[w * A_TILE + j - 1]; kp.x[w] = skx[w * A_TILE + j - 1]; }
+                h = hdiff<NW>(kp, kj);
+            }
+            unsigned cls = 0;
+            for (int i = 0; i < g.k; ++i) cls |= (unsigned)key_bit<NW>(kj, g.level[i]) << i;
+            sh[j] = (unsigned char)h;
+            B.meta[base + j] = (unsigned)h | (cls << 8);
+        }
+        __syncthreads();
+        for (int tau = 0; tau < ntau; ++tau) {
+            const int thr = tau_value(g, tau);
+            int mn = 0x7fff, mx = -1;
+            for (int j = tid; j < total; j += A_THREADS) {
+                if (j > 0 && (int)sh[j] >= thr) { mn = min(mn, j); mx = max(mx, j); }
+            }
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+            }
+            if (lane == 0 && mx >= 0) { atomicMin(&s_first[tau], mn); atomicMax(&s_last[tau], mx); }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            TileAggA *A = B.aggA + t;
+            A->count = total;
+            if (total > 0) {
+#pragma unroll
+                for (int w = 0; w < NW; ++w) {
+                    A->first[w] = skz[w * A_TILE];
+                    A->first[2 + w] = skx[w * A_TILE];
+                    A->last[w] = skz[w * A_TILE + total - 1];
+                    A->last[2 + w] = skx[w * A_TILE + total - 1];
+                }
+            }
+        }
+        if (tid < TAU_MAX) {
+            B.aggA[t].firstpos[tid] = (short)s_first[tid];
+            B.aggA[t].lastpos[tid] = (short)s_last[tid];
+        }
+        __syncthreads();
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ Key<NW> agg_key(const u64 *w4) {
+    Key<NW> k;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) { k.z[w] = w4[w]; k.x[w] = w4[2 + w]; }
+    return k;
+}
+
+// ---------------------------------------------------------------- A2 tilescan
+constexpr int S_THREADS = 1024;
+
+template <int NW>
+__global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
+    DevState *S = B.S;
+    if (S->err) return;
+    const long long rot = S->rot;
+    if (rot >= S->rot_end) return;
+    __shared__ GenRec g;
+    __shared__ long long sml[S_THREADS / 32 + 1];
+    __shared__ int smi[S_THREADS / 32 + 1];
+    const int tid = threadIdx.x;
+    if (tid == 0) g = B.gens[rot];
+    __syncthreads();
+    const long long n = S->n;
+    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    const int tpt = (ntiles + S_THREADS - 1) / S_THREADS;
+    const int t0 = min(tid * tpt, ntiles), t1 = min(t0 + tpt, ntiles);
+    // tile offsets
+    long long loc = 0;
+    for (int t = t0; t < t1; ++t) loc += B.aggA[t].count;
+    long long total;
+    long long run = block_excl_scan<S_THREADS>(loc, 0ll, OpSum(), sml, &total);
+    for (int t = t0; t < t1; ++t) { B.offA[t] = (int)run; run += B.aggA[t].count; }
+    if (n + total > B.cap) {
+        if (tid == 0) { S->err |= ERR_OVERFLOW; S->need = n + total; }
+        return;
+    }
+    if (tid == 0) S->a = total;
+    // first-element h of every tile: against the last key of the previous non-empty tile
+    int lastne = -1;
+    for (int t = t0; t < t1; ++t) if (B.aggA[t].count > 0) lastne = t;
+    int tot_i;
+    int carry = block_excl_scan<S_THREADS>(lastne, -1, OpMax(), smi, &tot_i);
+    for (int t = t0; t < t1; ++t) {
+        int hf = -1;
+        if (B.aggA[t].count > 0) {
+            hf = carry >= 0 ? hdiff<NW>(agg_key<NW>(B.aggA[carry].last), agg_key<NW>(B.aggA[t].first)) : H_INF;
+            carry = t;
+        }
+        B.hfirstA[t] = hf;
+    }
+    __syncthreads();
+    const int ntau = 2 * g.k;
+    const int itotal = (int)total;
+    for (int tau = 0; tau < ntau; ++tau) {
+        const int thr = tau_value(g, tau);
+        // forward: last global position with h >= thr, strictly before each tile
+        int lm = -1;
+        for (int t = t0; t < t1; ++t) {
+            const int cnt = B.aggA[t].count;
+            if (cnt == 0) continue;
+            int L = B.hfirstA[t] >= thr ? B.offA[t] : -1;
+            const int lp = B.aggA[t].lastpos[tau];
+            if (lp >= 0) L = max(L, B.offA[t] + lp);
+            lm = max(lm, L);
+        }
+        int cf = block_excl_scan<S_THREADS>(lm, -1, OpMax(), smi, &tot_i);
+        for (int t = t0; t < t1; ++t) {
+            B.fwdA[(long long)t * TAU_MAX + tau] = cf;
+            const int cnt = B.aggA[t].count;
+            if (cnt == 0) continue;
+            int L = B.hfirstA[t] >= thr ? B.offA[t] : -1;
+            const int lp = B.aggA[t].lastpos[tau];
+            if (lp >= 0) L = max(L, B.offA[t] + lp);
+            cf = max(cf, L);
+        }
+        // backward: first global position with h >= thr, strictly after each tile
+        int fm = 0x7fffffff;
+        for (int t = t0; t < t1; ++t) {
+            const int cnt = B.aggA[t].count;
+            if (cnt == 0) continue;
+            int F = 0x7fffffff;
+            const int fp = B.aggA[t].firstpos[tau];
+            if (fp != 0x7fff) F = B.offA[t] + fp;
+            if (B.hfirstA[t] >= thr) F = B.offA[t];
+            fm = min(fm, F);
+        }
+        int cb = block_excl_suffix<S_THREADS>(fm, 0x7fffffff, OpMin(), smi);
+        for (int t = t1 - 1; t >= t0; --t) {
+            B.bwdA[(long long)t * TAU_MAX + tau] = min(cb, itotal);
+            const int cnt = B.aggA[t].count;
+            if (cnt == 0) continue;
+            int F = 0x7fffffff;
+            const int fp = B.aggA[t].firstpos[tau];
+            if (fp != 0x7fff) F = B.offA[t] + fp;
+            if (B.hfirstA[t] >= thr) F = B.offA[t];
+            cb = min(cb, F);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- A3 permute
+template <int NW>
+__global__ void __launch_bounds__(A_THREADS) k_permute(Bufs B) {
+    DevState *S = B.S;
+    if (S->err) return;
+    const long long rot = S->rot;
+    if (rot >= S->rot_end) return;
+    __shared__ GenRec g;
+    __shared__ unsigned smeta[A_TILE];
+    __shared__ int ssrc[A_TILE];
+    __shared__ int sscan[A_THREADS / 32 + 1];
+    const int tid = threadIdx.x;
+    if (tid == 0) g = B.gens[rot];
+    __syncthreads();
+    const long long n = S->n;
+    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int cnt = B.aggA[t].count;
+        if (cnt == 0) continue;
+        const int off = B.offA[t];
+        const long long base = (long long)t * A_TILE;
+        for (int j = tid; j < cnt; j += A_THREADS) { smeta[j] = B.meta[base + j]; ssrc[j] = B.srcidx[base + j]; }
+        __syncthreads();
+        const int j0 = tid * A_ITEMS;
+        int h[A_ITEMS];
+        unsigned cls[A_ITEMS];
+        int delta[A_ITEMS];
+#pragma unroll
+        for (int q = 0; q < A_ITEMS; ++q) {
+            const int j = j0 + q;
+            const bool valid = j < cnt;
+            h[q] = valid ? (j == 0 ? B.hfirstA[t] : (int)(smeta[j] & 0xffu)) : -1;
+            cls[q] = valid ? (smeta[j] >> 8) : 0u;
+            delta[q] = 0;
+        }
+        for (int i = 0; i < g.k; ++i) {
+            int fw[2][A_ITEMS], bw[2][A_ITEMS];
+#pragma unroll
+            for (int sel = 0; sel < 2; ++sel) {
+                const int tau = 2 * i + sel;
+                const int thr = tau_value(g, tau);
+                int run = -1;
+#pragma unroll
+                for (int q = 0; q < A_ITEMS; ++q) { if (h[q] >= thr) run = off + j0 + q; fw[sel][q] = run; }
+                int tot;
+                int cf = block_excl_scan<A_THREADS>(run, -1, OpMax(), sscan, &tot);
+                cf = max(cf, B.fwdA[(long long)t * TAU_MAX + tau]);
+#pragma unroll
+                for (int q = 0; q < A_ITEMS; ++q) fw[sel][q] = max(fw[sel][q], cf);
+                int runb = 0x7fffffff;
+#pragma unroll
+                for (int q = A_ITEMS - 1; q >= 0; --q) { bw[sel][q] = runb; if (h[q] >= thr) runb = off + j0 + q; }
+                int cb = block_excl_suffix<A_THREADS>(runb, 0x7fffffff, OpMin(), sscan);
+                cb = min(cb, B.bwdA[(long long)t * TAU_MAX + tau]);
+#pragma unroll
+                for (int q = 0; q < A_ITEMS; ++q) bw[sel][q] = min(bw[sel][q], cb);
+            }
+#pragma unroll
+            for (int q = 0; q < A_ITEMS; ++q) {
+                if ((cls[q] >> i) & 1u) delta[q] -= fw[0][q] - fw[1][q];
+                else delta[q] += bw[1][q] - bw[0][q];
+            }
+        }
+        const long long atot = S->a;
+#pragma unroll
+        for (int q = 0; q < A_ITEMS; ++q) {
+            const int j = j0 + q;
+            if (j < cnt) {
+                const long long pos = (long long)off + j + delta[q];
+                if (pos >= 0 && pos < atot) B.src[pos] = ssrc[j];
+                else atomicOr(&S->err, ERR_BOUNDS);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- merge inputs
+// MODE 0: structured window-1 rotation (V = live[src[k]] xor M, sin branch on the fly,
+//         live cos branch applied on load).
+// MODE 1: direct (V = sorted materialised appends; live already rotated).
+// MODE 2: filter only (no V): the order-preserving compaction of the clip family.
+template <int NW, int MODE>
+__device__ __forceinline__ Key<NW> v_key(const Bufs &B, const GenRec &g, const u64 *Z, const u64 *X, long long k) {
+    if constexpr (MODE == 0) {
+        int p = B.src[k];
+        if (p < 0 || p >= B.S->n) { atomicOr(&B.S->err, ERR_BOUNDS); p = 0; }
+        Key<NW> P = load_key<NW>(Z, X, p);
+#pragma unroll
+        for (int w = 0; w < NW; ++w) { P.z[w] ^= g.gz[w]; P.x[w] ^= g.gx[w]; }
+        return P;
+    } else {
+        return load_key<NW>(B.vz, B.vx, k);
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ long long v_count(const DevState *S) {
+    return MODE == 0 ? S->a : MODE == 1 ? S->an : 0ll;
+}
+
+// ---------------------------------------------------------------- P partition
+template <int NW, int MODE>
+__global__ void k_partition(Bufs B) {
+    DevState *S = B.S;
+    if (S->err) return;
+    if (MODE == 0 && S->rot >= S->rot_end) return;
+    GenRec g;
+    if constexpr (MODE == 0) g = B.gens[S->rot];
+    const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
+    const int cur = S->cur;
+    const u64 *Z = B.z[cur], *X = B.x[cur];
+    const long long nsplit = max(1ll, (tot + B_D - 1) / B_D);
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s <= nsplit; s += (long long)gridDim.x * blockDim.x) {
+        const long long d = min(s * (long long)B_D, tot);
+        long long lo = max(0ll, d - a), hi = min(d, n);
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            const Key<NW> lm = load_key<NW>(Z, X, mid);
+            const Key<NW> vm = v_key<NW, MODE>(B, g, Z, X, d - mid - 1);
+            if (!key_lt<NW>(vm, lm)) lo = mid + 1; else hi = mid;
+        }
+        long long i = lo, j = d - lo;
+        // keep an equal-key run (live element followed by its appends) in one tile
+        if (j < a && (i > 0 || j > 0)) {
+            Key<NW> last;
+            if (j > 0 && i > 0) {
+                const Key<NW> lv = load_key<NW>(Z, X, i - 1);
+                const Key<NW> vv = v_key<NW, MODE>(B, g, Z, X, j - 1);
+                last = key_lt<NW>(vv, lv) ? lv : vv;
+            } else if (j > 0) {
+                last = v_key<NW, MODE>(B, g, Z, X, j - 1);
+            } else {
+                last = load_key<NW>(Z, X, i - 1);
+            }
+            while (j < a && key_eq<NW>(v_key<NW, MODE>(B, g, Z, X, j), last)) ++j;
+        }
+        B.split_i[s] = (int)i;
+        B.split_j[s] = (int)j;
+    }
+}
+
+// ---------------------------------------------------------------- B merge
+template <int NW>
+constexpr size_t merge_smem_bytes() {
+    return (size_t)B_CAP * (2 * NW * 8 + 8 + 8 + 2 + 2 + 1) + 64;
+}
+
+// MODE 2 (clip family) filters with DevParams::clip; evolve modes with ::strict.
+template <int MODE>
+__device__ __forceinline__ const DevFilter &merge_filter(const DevParams &P) {
+    if constexpr (MODE == 2) return P.clip; else return P.strict;
+}
+
+template <int NW, int MODE>
+__global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
+    DevState *S = B.S;
+    if (S->err) return;
+    if (MODE == 0 && S->rot >= S->rot_end) return;
+    __shared__ GenRec g;
+    __shared__ int s_tile;
+    __shared__ int s_sc[B_THREADS / 32 + 1];
+    __shared__ double s_red[3][B_THREADS / 32];
+    __shared__ unsigned s_base;
+    extern __shared__ u64 sm[];
+    u64 *skz = sm;                                                    // [NW][B_CAP]
+    u64 *skx = skz + NW * B_CAP;                                      // [NW][B_CAP]
+    double *sval = reinterpret_cast<double *>(skx + NW * B_CAP);      // [B_CAP] merge inputs
+    double *sout = sval + B_CAP;                                      // [B_CAP] compacted outputs
+    unsigned short *sperm = reinterpret_cast<unsigned short *>(sout + B_CAP);  // [B_CAP]
+    unsigned short *sslot = sperm + B_CAP;                            // [B_CAP]
+    unsigned char *sdead = reinterpret_cast<unsigned char *>(sslot + B_CAP);   // [B_CAP]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (MODE == 0 && tid == 0) g = B.gens[S->rot];
+    __syncthreads();
+    const DevParams &P = *B.P;
+    const DevFilter &F = merge_filter<MODE>(P);
+    const int flags = MODE == 0 ? g.flags : argflags;
+    const bool do_chan = MODE != 2 && (flags & GEN_CHANNEL) != 0 && P.chan_kind >= 0;
+    const bool do_corr = MODE != 2 && P.corr_kind == 1;
+    const bool do_meas = (flags & GEN_MEASURE) != 0 || do_corr;
+    const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
+    const int cur = S->cur;
+    const u64 *Z = B.z[cur], *X = B.x[cur];
+    const double *C = B.c[cur];
+    u64 *OZ = B.z[cur ^ 1], *OX = B.x[cur ^ 1];
+    double *OC = B.c[cur ^ 1];
+    const int nsplit = (int)max(1ll, (tot + B_D - 1) / B_D);
+    const unsigned epoch = S->epoch;
+    const bool pref = MODE == 0 && n > S->acap_logical;
+    const u64 ket[2] = {P.ket[0], P.ket[1]};
+
+    auto skey = [&](int slot) {
+        Key<NW> k;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) { k.z[w] = skz[w * B_CAP + slot]; k.x[w] = skx[w * B_CAP + slot]; }
+        return k;
+    };
+
+    while (true) {
+        if (tid == 0) s_tile = atomicAdd(&S->b_tile_ctr, 1);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= nsplit) break;
+        const int i0 = B.split_i[t], j0 = B.split_j[t];
+        const int i1 = B.split_i[t + 1], j1 = B.split_j[t + 1];
+        int nl = i1 - i0, nv = j1 - j0;
+        const bool bad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
+        if (bad) { nl = 0; nv = 0; }
+        const int ntot = nl + nv;
+        // ---- stage the live part (cos branch / early-merge pre-filter) and the appended part
+        int nalive = 0;
+        for (int e = tid; e < nl; e += B_THREADS) {
+            const Key<NW> k = load_key<NW>(Z, X, i0 + e);
+            double c = C[i0 + e];
+            unsigned char dead = 0;
+            if constexpr (MODE == 0) {
+                Key<NW> q;
+                double sg;
+                const bool anti = rotate_term<NW>(k, g, &q, &sg);
+                if (pref && should_drop<NW>(P.strict, k, fabs(c))) dead = 1;
+                else if (anti) c = __dmul_rn(c, g.cosv);
+                nalive += dead ? 0 : 1;
+            }
+#pragma unroll
+            for (int w = 0; w < NW; ++w) { skz[w * B_CAP + e] = k.z[w]; skx[w * B_CAP + e] = k.x[w]; }
+            sval[e] = c;
+            sdead[e] = dead;
+        }
+        for (int e = tid; e < nv; e += B_THREADS) {
+            Key<NW> k;
+            double c;
+            if constexpr (MODE == 0) {
+                int p = B.src[j0 + e];
+                if (p < 0 || p >= n) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
+                const Key<NW> pk = load_key<NW>(Z, X, p);
+                double sg = 0.0;
+                rotate_term<NW>(pk, g, &k, &sg);
+                c = __dmul_rn(sg * g.sinv, C[p]);
+            } else {
+                k = load_key<NW>(B.vz, B.vx, j0 + e);
+                c = B.vc[j0 + e];
+            }
+#pragma unroll
+            for (int w = 0; w < NW; ++w) { skz[w * B_CAP + nl + e] = k.z[w]; skx[w * B_CAP + nl + e] = k.x[w]; }
+            sval[nl + e] = c;
+            sdead[nl + e] = 0;
+        }
+        __syncthreads();
+        // ---- merge path inside the tile; each thread owns a contiguous output range
+        // (live first on equal keys: spv_kernels.jl:338)
+        const int ipt = (ntot + B_THREADS - 1) / B_THREADS;
+        const int d0 = min(tid * ipt, ntot), dend = min(d0 + ipt, ntot);
+        if (d0 < dend) {
+            int lo = max(0, d0 - nv), hi = min(d0, nl);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (!key_lt<NW>(skey(nl + d0 - mid - 1), skey(mid))) lo = mid + 1; else hi = mid;
+            }
+            int i = lo, j = d0 - lo;
+            for (int d = d0; d < dend; ++d) {
+                bool takeL;
+                if (i >= nl) takeL = false;
+                else if (j >= nv) takeL = true;
+                else takeL = !key_lt<NW>(skey(nl + j), skey(i));
+                sperm[d] = (unsigned short)(takeL ? i++ : nl + j++);
+            }
+        }
+        __syncthreads();
+        // ---- reduce equal-key runs (live value first, then appends in order,
+        // spv_kernels.jl:338-350), strict filter on the unscaled sum, channel epilogue
+        int kept = 0;
+        double outv[B_IPTMAX];
+        unsigned short slotv[B_IPTMAX];
+        Neu e_keep{0.0, 0.0}, e_drop{0.0, 0.0}, e_pre{0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < B_IPTMAX; ++q) {
+            const int p = d0 + q;
+            if (p >= dend) break;
+            const int sl = sperm[p];
+            const Key<NW> kp = skey(sl);
+            if (p > 0 && key_eq<NW>(skey(sperm[p - 1]), kp)) continue;  // not a run head
+            double acc = 0.0;
+            bool have = false;
+            const bool diag = is_diag<NW>(kp);
+            const double sgn = diag ? ket_sign<NW>(kp, ket) : 0.0;
+            for (int r = p; r < ntot; ++r) {
+                const int sr = sperm[r];
+                if (r > p && !key_eq<NW>(skey(sr), kp)) break;
+                if (sdead[sr]) { if (diag && do_meas) e_pre.add(sgn * sval[sr]); continue; }
+                acc = have ? __dadd_rn(acc, sval[sr]) : sval[sr];
+                have = true;
+            }
+            if (!have) continue;
+            if (should_drop<NW>(F, kp, fabs(acc))) {
+                if (diag && do_meas) e_drop.add(sgn * acc);
+                continue;
+            }
+            const double o = do_chan ? __dmul_rn(acc, channel_factor<NW>(P, kp)) : acc;
+            if (diag && do_meas) e_keep.add(sgn * o);
+            outv[kept] = o;
+            slotv[kept] = (unsigned short)sl;
+            ++kept;
+        }
+        int tkept;
+        const int loff = block_excl_scan<B_THREADS>(kept, 0, OpSum(), s_sc, &tkept);
+        if (warp == 0) {
+            const unsigned ex = lookback_warp(B.tstat, t, epoch, (unsigned)tkept, &S->err);
+            if (lane == 0) s_base = ex;
+        }
+#pragma unroll
+        for (int q = 0; q < B_IPTMAX; ++q) if (q < kept) { sout[loff + q] = outv[q]; sslot[loff + q] = slotv[q]; }
+        __syncthreads();
+        const long long obase = s_base;
+        if (obase + tkept > B.cap) {
+            if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
+            tkept = 0;
+        }
+        for (int e = tid; e < tkept; e += B_THREADS) {
+            store_key<NW>(OZ, OX, obase + e, skey(sslot[e]));
+            OC[obase + e] = sout[e];
+        }
+        if (bad && tid == 0) atomicOr(&S->err, ERR_TILE);
+        if (MODE == 0 && pref) {
+            int na = nalive;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) na += __shfl_xor_sync(0xffffffffu, na, d);
+            if (lane == 0 && na) atomicAdd((unsigned long long *)&S->npref, (unsigned long long)na);
+        }
+        if (do_meas) {
+            double v0 = e_keep.s + e_keep.c, v1 = e_drop.s + e_drop.c, v2 = e_pre.s + e_pre.c;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                v0 += __shfl_xor_sync(0xffffffffu, v0, d);
+                v1 += __shfl_xor_sync(0xffffffffu, v1, d);
+                v2 += __shfl_xor_sync(0xffffffffu, v2, d);
+            }
+            if (lane == 0) { s_red[0][warp] = v0; s_red[1][warp] = v1; s_red[2][warp] = v2; }
+            __syncthreads();
+            if (tid < 3) {
+                double s = 0.0;
+                for (int w = 0; w < B_THREADS / 32; ++w) s += s_red[tid][w];
+                B.part[(long long)t * 4 + tid] = s;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Commits a merge launch (one block, after k_merge): new live count and buffer
+// parity, WindowCounters totals, the early-merge append-capacity rule
+// (spv_evolve.jl:356-362), the ordered reduction of <ket|O|ket> and correction
+// partials, and the reset of the tile dispenser.  Kept out of k_merge so that no
+// CTA of a merge launch can observe a half-committed state.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
+    DevState *S = B.S;
+    if (S->err & ~ERR_TIMEOUT) return;
+    if (MODE == 0 && S->rot >= S->rot_end) return;
+    __shared__ double s_p[3][256];
+    const int tid = threadIdx.x;
+    const DevParams &P = *B.P;
+    const int flags = MODE == 0 ? B.gens[S->rot].flags : argflags;
+    const bool do_corr = MODE != 2 && P.corr_kind == 1;
+    const bool do_meas = (flags & GEN_MEASURE) != 0 || do_corr;
+    const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
+    const int nsplit = (int)max(1ll, (tot + B_D - 1) / B_D);
+    if (do_meas) {
+        const int per = (nsplit + 255) / 256;
+        Neu r0{0, 0}, r1{0, 0}, r2{0, 0};
+        for (int tt = tid * per; tt < min(nsplit, (tid + 1) * per); ++tt) {
+            r0.add(B.part[(long long)tt * 4 + 0]);
+            r1.add(B.part[(long long)tt * 4 + 1]);
+            r2.add(B.part[(long long)tt * 4 + 2]);
+        }
+        s_p[0][tid] = r0.s + r0.c; s_p[1][tid] = r1.s + r1.c; s_p[2][tid] = r2.s + r2.c;
+        __syncthreads();
+        if (tid == 0) {
+            Neu f0{0, 0}, f1{0, 0}, f2{0, 0};
+            for (int w = 0; w < 256; ++w) { f0.add(s_p[0][w]); f1.add(s_p[1][w]); f2.add(s_p[2][w]); }
+            S->expect_val = f0.s + f0.c;
+            S->measure_valid = 1;
+            if (do_corr) S->corr_energy = __dsub_rn(S->corr_energy, __dadd_rn(f1.s + f1.c, f2.s + f2.c));
+        }
+    }
+    if (tid == 0) {
+        const bool pref = MODE == 0 && n > S->acap_logical;
+        const u64 st = st_load(B.tstat + (nsplit - 1));
+        const long long total = (long long)(unsigned)(st & 0xffffffffu);
+        S->n = total;
+        S->cur ^= 1;
+        S->merge_in += tot;
+        S->merge_out += total;
+        if (total > S->peak) S->peak = total;
+        if (MODE == 0) {
+            S->live_in += n;
+            S->created += a;
+            if (pref) {
+                S->early += 1;
+                const long long np = S->npref;
+                if (np > S->acap_logical) S->acap_logical = max(2 * S->acap_logical, np);
+                S->npref = 0;
+            }
+            S->rot += 1;
+        }
+        if (MODE == 1) S->an = 0;
+        S->b_tile_ctr = 0;
+        S->epoch += 1;
+    }
+}
+
+}  // namespace pp

@@ -1,0 +1,130 @@
+"""ctypes binding of libpauliprop.so (include/pauliprop.h).
+
+The library is built in-tree (paulioperators.jl_b200/lib/libpauliprop.so by
+``make -C paulioperators.jl_b200``).  There is no CPU fallback: if the library
+is missing, importing this module raises, and on a machine without a CUDA
+device every compute entry point returns PP_DEVICE_ERROR, which is raised as
+``DeviceError``.
+"""
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpauliprop.so")
+
+PP_OK = 0
+PP_ARGUMENT_ERROR = 1
+PP_DIMENSION_MISMATCH = 2
+PP_ERROR_EXCEPTION = 3
+PP_OUT_OF_MEMORY = 4
+PP_DEVICE_ERROR = 5
+PP_TIMEOUT = 6
+PP_NOT_IMPLEMENTED = 7
+
+
+class ArgumentError(ValueError):
+    """Julia ArgumentError (bad probability, qubit index, window, strategy kind)."""
+
+
+class DimensionMismatch(ValueError):
+    """Julia DimensionMismatch (generators and angles of different length)."""
+
+
+class PauliPropError(RuntimeError):
+    """Julia ErrorException (N > 128, complex coefficient for real storage, broken invariant)."""
+
+
+class DeviceError(RuntimeError):
+    """CUDA runtime failure, or no CUDA device present."""
+
+
+class PPFilter(Structure):
+    """pp_filter == the reference's isbits MergeFilter (spv_kernels.jl:33-42)."""
+    _fields_ = [("wmax", c_int64), ("xwmax", c_int64), ("mwmax", c_int64),
+                ("thresh", c_double), ("alpha_w", c_double), ("dthresh_w", c_double),
+                ("alpha_xw", c_double), ("dthresh_xw", c_double)]
+
+
+class PPCounters(Structure):
+    _fields_ = [("nwin", c_int64),
+                ("terms_created", POINTER(c_int64)), ("merge_in", POINTER(c_int64)),
+                ("merge_out", POINTER(c_int64)), ("early_merges", POINTER(c_int64)),
+                ("t_rotate", POINTER(c_double)), ("t_merge", POINTER(c_double))]
+
+
+class PPEvolveOpts(Structure):
+    _fields_ = [("window", c_int64),
+                ("strict", POINTER(PPFilter)), ("local", POINTER(PPFilter)),
+                ("strict_kind", c_int32), ("corr_kind", c_int32),
+                ("adapt_max_terms", c_int64), ("adapt_min_thresh", c_double),
+                ("ket", c_void_p), ("corr_energy", POINTER(c_double)),
+                ("counters", POINTER(PPCounters)),
+                ("chan_kind", c_int32), ("pad", c_int32),
+                ("chan_prm", c_double * 3), ("chan_mask", c_void_p),
+                ("expect_out", POINTER(c_double)),
+                ("chan_every", c_int64), ("stats_out", POINTER(c_double)),
+                ("profile", c_int32), ("pad2", c_int32)]
+
+
+PP_STATS_LEN = 16
+STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
+        "t_rotate": 6, "t_merge": 7, "launches": 8, "t_partition": 9}
+
+
+# Every symbol include/pauliprop.h declares, with its ctypes signature.
+SIGNATURES = {
+    "pp_create": (c_int32, [c_int32, c_int64, c_int64, POINTER(c_void_p)]),
+    "pp_destroy": (c_int32, [c_void_p]),
+    "pp_upload": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32]),
+    "pp_download": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]),
+    "pp_length": (c_int32, [c_void_p, POINTER(c_int64)]),
+    "pp_copy": (c_int32, [c_void_p, POINTER(c_void_p)]),
+    "pp_evolve1": (c_int32, [c_void_p, c_void_p, c_void_p, c_double, c_double]),
+    "pp_evolve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPEvolveOpts)]),
+    "pp_compact": (c_int32, [c_void_p, POINTER(PPFilter)]),
+    "pp_adaptive": (c_int32, [c_void_p, c_int64, c_double]),
+    "pp_channel": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
+    "pp_expect_ket": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
+    "pp_check": (c_int32, [c_void_p, POINTER(c_int32)]),
+    "pp_stream": (c_int32, [c_void_p, POINTER(c_void_p)]),
+    "pp_device_bytes": (c_int32, [c_void_p, POINTER(c_int64)]),
+    "pp_power_table": (c_int32, [c_double, c_int32, c_void_p]),
+    "pp_last_error": (c_char_p, []),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libpauliprop.so not found at {LIB_PATH}; build it with "
+            "`make -C paulioperators.jl_b200` (there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status):
+    """Raise the Python analogue of the reference's exception for a pp_status."""
+    if status == PP_OK:
+        return
+    msg = (lib.pp_last_error() or b"").decode(errors="replace")
+    if status == PP_ARGUMENT_ERROR:
+        raise ArgumentError(msg)
+    if status == PP_DIMENSION_MISMATCH:
+        raise DimensionMismatch(msg)
+    if status == PP_ERROR_EXCEPTION:
+        raise PauliPropError(msg)
+    if status == PP_OUT_OF_MEMORY:
+        raise MemoryError(msg)
+    if status == PP_TIMEOUT:
+        raise TimeoutError(msg)
+    if status == PP_NOT_IMPLEMENTED:
+        raise NotImplementedError(msg)
+    raise DeviceError(msg)

@@ -1,0 +1,87 @@
+"""Host-side logic: strategy compilation (spv_kernels.jl:81-125), Pauli strings,
+qubit masks, and the seeded workload generators."""
+import math
+
+import pytest
+
+import pauliprop as pp
+from pauliprop import circuits
+from pauliprop.paulis import INT64_MAX
+
+
+def test_compile_filters():
+    assert pp.compile_filter(pp.NoTruncation()) == pp.NOFILTER
+    f = pp.compile_filter(pp.CompositeTruncation(pp.CoeffTruncation(1e-5), pp.WeightTruncation(12)))
+    assert f.thresh == 1e-5 and f.wmax == 12 and f.xwmax == INT64_MAX and f.dthresh_w < 0
+    f = pp.compile_filter(pp.CompositeTruncation(pp.WeightDampedTruncation(0.5, 1e-3),
+                                                 pp.XWeightDampedTruncation(0.2, 1e-4), pp.WeightTruncation(4)))
+    assert (f.alpha_w, f.dthresh_w, f.alpha_xw, f.dthresh_xw, f.wmax) == (0.5, 1e-3, 0.2, 1e-4, 4)
+    with pytest.raises(RuntimeError):
+        pp.combine_filters(pp.compile_filter(pp.WeightDampedTruncation(0.5)),
+                           pp.compile_filter(pp.WeightDampedTruncation(0.6)))
+    assert pp.is_compilable(pp.CompositeTruncation(pp.WeightTruncation(2), pp.CoeffTruncation(1e-4)))
+    assert not pp.is_compilable(pp.AdaptiveTruncation(10, 1e-12))
+    assert not pp.is_compilable(pp.CompositeTruncation(pp.WeightDampedTruncation(0.5), pp.WeightDampedTruncation(0.1)))
+    assert not pp.is_compilable(pp.StochasticCoeffTruncation(0.1))
+
+
+def test_default_constructors():
+    # test_truncation.jl:347-355
+    assert pp.CoeffTruncation().thresh == 1e-6
+    assert pp.WeightDampedTruncation(0.5).thresh == 1e-6
+    assert pp.XWeightDampedTruncation(0.5).alpha == 0.5
+    assert pp.AdaptiveTruncation(max_terms=100, min_thresh=1e-6).max_terms == 100
+    assert isinstance(pp.CompositeTruncation([pp.NoTruncation(), pp.CoeffTruncation(0.1)]).strategies, tuple)
+
+
+def test_pauli_strings():
+    b = pp.PauliBasis.from_string("XYZI")
+    assert (b.z, b.x) == (0b0110, 0b0011)
+    assert str(b) == "XYZI"
+    assert pp.PauliBasis.from_sites(4, X=[1], Y=[2], Z=[3]) == b
+    with pytest.raises(ValueError):
+        pp.PauliBasis.from_string("XQ")
+
+
+def test_qubit_mask():
+    assert pp.qubit_mask(3, None) == 0b111
+    assert pp.qubit_mask(3, [1, 3]) == 0b101
+    assert pp.qubit_mask(3, 2) == 0b010
+    for bad in ([0], [4], 4):
+        with pytest.raises(pp.ArgumentError):
+            pp.qubit_mask(3, bad)
+
+
+def test_workloads():
+    w1 = circuits.chain20()
+    assert w1.N == 20 and w1.rotations == 8 * 39 and w1.observable == [(1 << 9, 0, 1.0)]
+    w2 = circuits.lattice64()
+    assert w2.rotations == 20 * 176 and len(w2.observable) == 64 and w2.wmax == 12
+    assert len(circuits.lattice_edges()) == 112
+    w3 = circuits.random_graph127()
+    edges = w3.meta["edges"]
+    assert len(edges) == 144 and w3.rotations == 24 * 271
+    deg = {}
+    for i, j in edges:
+        deg[i] = deg.get(i, 0) + 1
+        deg[j] = deg.get(j, 0) + 1
+    assert max(deg.values()) <= 3
+    assert all(0.1 <= a <= 0.5 for a in w3.angles[:144]) and all(0 <= a <= math.pi / 4 for a in w3.angles[144:])
+    assert circuits.random_graph127().angles == w3.angles  # deterministic seed
+    b = circuits.batch_instances(16)
+    assert all(4 <= x.layers <= 24 for x in b)
+    assert all(1 <= bin(x.observable[0][0] | x.observable[0][1]).count("1") <= 4 for x in b)
+
+
+def test_splitmix_reference_values():
+    # splitmix64 seeded with 0: published first outputs
+    r = circuits.SplitMix64(0)
+    assert r.next_u64() == 0xE220A8397B1DCDAF
+    assert r.next_u64() == 0x6E789E6AA1B965F4
+
+
+def test_trotterize_order2():
+    terms = circuits.heisenberg_chain_terms(4)
+    g, a = circuits.trotterize(terms, 0.1, n_trotter=2, order=2)
+    assert len(g) == 2 * 2 * len(terms)
+    assert g[len(terms)] == terms[-1][0] and a[0] == pytest.approx(0.05 * terms[0][1])
