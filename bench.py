@@ -310,8 +310,6 @@ def run_ours(args):
     hz = torch.from_numpy(obs_z.copy()).pin_memory()
     hx = torch.from_numpy(obs_x.copy()).pin_memory()
     hc = torch.from_numpy(obs_c.copy()).pin_memory()
-    nfin = len(g)
-    oz = torch.empty((max(nfin, 1), nw), dtype=torch.uint64).pin_memory() if hasattr(torch, "uint64") else None
     h2d = d2h = 0
     te = []
     for _ in range(args.steps):

@@ -43,6 +43,7 @@ def key_of(s):
 
 
 def rand_terms(rng, N, n, real=True, scale=1.0):
+    n = min(n, 4**N // 2)   # never ask for more distinct keys than the space holds
     out = {}
     while len(out) < n:
         out[(rng.getrandbits(N), rng.getrandbits(N))] = scale * (rng.random() - 0.5)

@@ -343,7 +343,7 @@ def test_config1_chain20_full():
     g, v = run_workload(w, w.layers)
     compare(g, v, bitexact=True)
     assert abs(pp.expectation_value(g, 0) - v.expect(0)) <= expect_bound(v)
-    assert len(g) > 1000
+    assert len(g) > 100
 
 
 @pytest.mark.parametrize("fused", [True, False])
