@@ -45,7 +45,7 @@ extern "C" const char *pp_last_error(void) { return g_err.c_str(); }
     } while (0)
 
 static const pp_filter NOFILTER_H = {INT64_MAX, INT64_MAX, INT64_MAX, -1.0, 0.0, -1.0, 0.0, -1.0};
-static constexpr int CHUNK_ROT = 32;   // rotations launched between state read-backs
+static constexpr int CHUNK_ROT = 64;   // rotations launched between state read-backs
 
 struct pp_spv {
     int N = 0, NW = 1, dev = 0, nsm = 148;
@@ -79,6 +79,9 @@ struct pp_spv {
     int occA1 = 1, occA3 = 1, occB = 1, occG = 1;
     long long bytes = 0;
     long long acap_logical_init = 16;
+    long long buf_gen = 0;                 // bumped by every (re)allocation
+    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+    long long gexec_gen[3] = {-1, -1, -1};
 };
 
 // ------------------------------------------------------------------ helpers
@@ -93,6 +96,7 @@ static int dalloc(pp_spv *h, T **p, long long count) {
         return fail(PP_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
     h->bytes += (long long)count * sizeof(T);
+    h->buf_gen++;
     return PP_OK;
 }
 
@@ -405,7 +409,7 @@ static void launch_struct_rotation(pp_spv *h, const Bufs &B) {
     k_classify<NW><<<h->nsm * h->occA1, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE, s>>>(B);
     k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
     k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
-    k_partition<NW, 0><<<h->nsm * 4, 256, 0, s>>>(B);
+    k_partition<NW, 0><<<h->nsm * 4, P_THREADS, 0, s>>>(B);
     k_merge<NW, 0><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, 0);
     k_commit<0><<<1, 256, 0, s>>>(B, 0);
 }
@@ -413,7 +417,7 @@ static void launch_struct_rotation(pp_spv *h, const Bufs &B) {
 template <int NW, int MODE>
 static void launch_merge(pp_spv *h, const Bufs &B, int flags) {
     cudaStream_t s = h->stream;
-    k_partition<NW, MODE><<<h->nsm * 4, 256, 0, s>>>(B);
+    k_partition<NW, MODE><<<h->nsm * 4, P_THREADS, 0, s>>>(B);
     k_merge<NW, MODE><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, flags);
     k_commit<MODE><<<1, 256, 0, s>>>(B, flags);
 }
@@ -510,6 +514,7 @@ extern "C" int pp_destroy(pp_spv *h) {
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
                     h->S, h->P, h->gens};
     for (void *p : ptrs) if (p) cudaFree(p);
+    for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
     if (h->gens_h) cudaFreeHost(h->gens_h);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -603,6 +608,26 @@ static int ensure_gens(pp_spv *h, long long L) {
     return PP_OK;
 }
 
+// CUDA graph of `len` consecutive window-1 rotations (6 kernels each).  The
+// kernels take only buffer pointers and read the rotation cursor, counts and
+// parity from DevState, so one instantiated graph serves every chunk until a
+// buffer is reallocated.
+template <int NW>
+static int struct_graph(pp_spv *h, int gi, int len) {
+    if (h->gexec[gi] && h->gexec_gen[gi] == h->buf_gen) return PP_OK;
+    if (h->gexec[gi]) { cudaGraphExecDestroy(h->gexec[gi]); h->gexec[gi] = nullptr; }
+    Bufs B = make_bufs(h);
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < len; ++r) launch_struct_rotation<NW>(h, B);
+    CU(cudaStreamEndCapture(h->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&h->gexec[gi], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    h->gexec_gen[gi] = h->buf_gen;
+    return PP_OK;
+}
+
 // Per-call accounting of launches and (when profiling) per-kernel device time.
 struct RunProf {
     bool on = false;
@@ -621,10 +646,20 @@ static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
-        for (long long r = done; r < end; ++r) {
-            if (!timed) {
-                launch_struct_rotation<NW>(h, B);
-            } else {
+        if (!timed) {
+            // replay captured chunks: CHUNK_ROT, then 8, then single rotations
+            long long r = done;
+            while (r < end) {
+                const int gi = (end - r >= CHUNK_ROT) ? 0 : (end - r >= 8) ? 1 : 2;
+                const int len = gi == 0 ? CHUNK_ROT : gi == 1 ? 8 : 1;
+                TRY(struct_graph<NW>(h, gi, len));
+                CU(cudaGraphLaunch(h->gexec[gi], s));
+                r += len;
+                prof->launches += 6 * len;
+            }
+        }
+        for (long long r = done; r < end && timed; ++r) {
+            {
                 cudaEvent_t e[5];
                 for (int q = 0; q < 5; ++q) cudaEventCreate(&e[q]);
                 cudaEventRecord(e[0], s);
@@ -632,7 +667,7 @@ static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
                 k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
                 k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
                 cudaEventRecord(e[1], s);
-                k_partition<NW, 0><<<h->nsm * 4, 256, 0, s>>>(B);
+                k_partition<NW, 0><<<h->nsm * 4, P_THREADS, 0, s>>>(B);
                 cudaEventRecord(e[2], s);
                 k_merge<NW, 0><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, 0);
                 cudaEventRecord(e[3], s);

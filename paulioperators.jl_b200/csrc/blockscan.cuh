@@ -81,6 +81,78 @@ __device__ __forceinline__ T block_excl_suffix(T v, T identity, Op op, T *sm) {
     return res;
 }
 
+// Vector variants: NV independent scans sharing one set of barriers.  sm must
+// hold NV * (THREADS/32) ints.  Only the first `nact` components are scanned.
+template <int THREADS, int NV, typename Op>
+__device__ __forceinline__ void block_excl_scan_vec(int (&v)[NV], int identity, Op op, int *sm, int nact) {
+    constexpr int NWARP = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        if (c < nact) {
+            incl[c] = warp_incl_scan(v[c], op);
+            if (lane == 31) sm[c * NWARP + warp] = incl[c];
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            if (c < nact) {
+                int w = lane < NWARP ? sm[c * NWARP + lane] : identity;
+                int wi = warp_incl_scan(w, op);
+                if (lane < NWARP) sm[c * NWARP + lane] = wi;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        if (c < nact) {
+            int ex = __shfl_up_sync(0xffffffffu, incl[c], 1);
+            if (lane == 0) ex = identity;
+            v[c] = op(warp == 0 ? identity : sm[c * NWARP + warp - 1], ex);
+        }
+    }
+    __syncthreads();
+}
+
+template <int THREADS, int NV, typename Op>
+__device__ __forceinline__ void block_excl_suffix_vec(int (&v)[NV], int identity, Op op, int *sm, int nact) {
+    constexpr int NWARP = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        if (c < nact) {
+            incl[c] = warp_incl_suffix(v[c], op);
+            if (lane == 0) sm[c * NWARP + warp] = incl[c];
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            if (c < nact) {
+                int w = lane < NWARP ? sm[c * NWARP + lane] : identity;
+                int wi = warp_incl_suffix(w, op);
+                if (lane < NWARP) sm[c * NWARP + lane] = wi;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        if (c < nact) {
+            int ex = __shfl_down_sync(0xffffffffu, incl[c], 1);
+            if (lane == 31) ex = identity;
+            v[c] = op(warp == NWARP - 1 ? identity : sm[c * NWARP + warp + 1], ex);
+        }
+    }
+    __syncthreads();
+}
+
 struct OpSum { template <typename T> __device__ __forceinline__ T operator()(T a, T b) const { return a + b; } };
 struct OpMax { template <typename T> __device__ __forceinline__ T operator()(T a, T b) const { return a > b ? a : b; } };
 struct OpMin { template <typename T> __device__ __forceinline__ T operator()(T a, T b) const { return a < b ? a : b; } };

@@ -48,6 +48,8 @@ struct Bufs {
     const GenRec *gens;
 };
 
+constexpr int TAUV = 8;   // scan thresholds sharing one vector block scan
+
 __device__ __forceinline__ int tau_value(const GenRec &g, int tau) {
     return (int)g.level[tau >> 1] + (tau & 1);
 }
@@ -212,6 +214,7 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     __shared__ GenRec g;
     __shared__ long long sml[S_THREADS / 32 + 1];
     __shared__ int smi[S_THREADS / 32 + 1];
+    __shared__ int svec[TAUV * (S_THREADS / 32)];
     const int tid = threadIdx.x;
     if (tid == 0) g = B.gens[rot];
     __syncthreads();
@@ -246,56 +249,68 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     __syncthreads();
     const int ntau = 2 * g.k;
     const int itotal = (int)total;
-    for (int tau = 0; tau < ntau; ++tau) {
-        const int thr = tau_value(g, tau);
-        // forward: last global position with h >= thr, strictly before each tile
-        int lm = -1;
+    // Per threshold tau: forward = last global position with h >= tau strictly
+    // before each tile; backward = first such position strictly after it.  The
+    // thresholds of a group share one vector scan in each direction.
+    auto tileL = [&](int t, int tau, int thr) {
+        int L = B.hfirstA[t] >= thr ? B.offA[t] : -1;
+        const int lp = B.aggA[t].lastpos[tau];
+        if (lp >= 0) L = max(L, B.offA[t] + lp);
+        return L;
+    };
+    auto tileF = [&](int t, int tau, int thr) {
+        if (B.hfirstA[t] >= thr) return B.offA[t];
+        const int fp = B.aggA[t].firstpos[tau];
+        return fp != 0x7fff ? B.offA[t] + fp : 0x7fffffff;
+    };
+    for (int g0 = 0; g0 < ntau; g0 += TAUV) {
+        const int na = min(TAUV, ntau - g0);
+        int lm[TAUV], fm[TAUV];
+#pragma unroll
+        for (int c = 0; c < TAUV; ++c) { lm[c] = -1; fm[c] = 0x7fffffff; }
         for (int t = t0; t < t1; ++t) {
-            const int cnt = B.aggA[t].count;
-            if (cnt == 0) continue;
-            int L = B.hfirstA[t] >= thr ? B.offA[t] : -1;
-            const int lp = B.aggA[t].lastpos[tau];
-            if (lp >= 0) L = max(L, B.offA[t] + lp);
-            lm = max(lm, L);
+            if (B.aggA[t].count == 0) continue;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    const int thr = tau_value(g, g0 + c);
+                    lm[c] = max(lm[c], tileL(t, g0 + c, thr));
+                    fm[c] = min(fm[c], tileF(t, g0 + c, thr));
+                }
+            }
         }
-        int cf = block_excl_scan<S_THREADS>(lm, -1, OpMax(), smi, &tot_i);
+        block_excl_scan_vec<S_THREADS, TAUV>(lm, -1, OpMax(), svec, na);
+        block_excl_suffix_vec<S_THREADS, TAUV>(fm, 0x7fffffff, OpMin(), svec, na);
         for (int t = t0; t < t1; ++t) {
-            B.fwdA[(long long)t * TAU_MAX + tau] = cf;
-            const int cnt = B.aggA[t].count;
-            if (cnt == 0) continue;
-            int L = B.hfirstA[t] >= thr ? B.offA[t] : -1;
-            const int lp = B.aggA[t].lastpos[tau];
-            if (lp >= 0) L = max(L, B.offA[t] + lp);
-            cf = max(cf, L);
+            const bool ne = B.aggA[t].count > 0;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    B.fwdA[(long long)t * TAU_MAX + g0 + c] = lm[c];
+                    if (ne) lm[c] = max(lm[c], tileL(t, g0 + c, tau_value(g, g0 + c)));
+                }
+            }
         }
-        // backward: first global position with h >= thr, strictly after each tile
-        int fm = 0x7fffffff;
-        for (int t = t0; t < t1; ++t) {
-            const int cnt = B.aggA[t].count;
-            if (cnt == 0) continue;
-            int F = 0x7fffffff;
-            const int fp = B.aggA[t].firstpos[tau];
-            if (fp != 0x7fff) F = B.offA[t] + fp;
-            if (B.hfirstA[t] >= thr) F = B.offA[t];
-            fm = min(fm, F);
-        }
-        int cb = block_excl_suffix<S_THREADS>(fm, 0x7fffffff, OpMin(), smi);
         for (int t = t1 - 1; t >= t0; --t) {
-            B.bwdA[(long long)t * TAU_MAX + tau] = min(cb, itotal);
-            const int cnt = B.aggA[t].count;
-            if (cnt == 0) continue;
-            int F = 0x7fffffff;
-            const int fp = B.aggA[t].firstpos[tau];
-            if (fp != 0x7fff) F = B.offA[t] + fp;
-            if (B.hfirstA[t] >= thr) F = B.offA[t];
-            cb = min(cb, F);
+            const bool ne = B.aggA[t].count > 0;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    B.bwdA[(long long)t * TAU_MAX + g0 + c] = min(fm[c], itotal);
+                    if (ne) fm[c] = min(fm[c], tileF(t, g0 + c, tau_value(g, g0 + c)));
+                }
+            }
         }
     }
 }
 
 // ---------------------------------------------------------------- A3 permute
+// Thresholds are processed in groups of TAUV: per group one vector forward
+// max-scan and one vector backward min-scan of per-thread aggregates, then each
+// thread re-scans its A_ITEMS items in registers.
+
 template <int NW>
-__global__ void __launch_bounds__(A_THREADS) k_permute(Bufs B) {
+__global__ void __launch_bounds__(A_THREADS, 2) k_permute(Bufs B) {
     DevState *S = B.S;
     if (S->err) return;
     const long long rot = S->rot;
@@ -303,12 +318,14 @@ __global__ void __launch_bounds__(A_THREADS) k_permute(Bufs B) {
     __shared__ GenRec g;
     __shared__ unsigned smeta[A_TILE];
     __shared__ int ssrc[A_TILE];
-    __shared__ int sscan[A_THREADS / 32 + 1];
+    __shared__ int sscan[TAUV * (A_THREADS / 32)];
     const int tid = threadIdx.x;
     if (tid == 0) g = B.gens[rot];
     __syncthreads();
     const long long n = S->n;
+    const long long atot = S->a;
     const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    const int ntau = 2 * g.k;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int cnt = B.aggA[t].count;
         if (cnt == 0) continue;
@@ -328,35 +345,54 @@ __global__ void __launch_bounds__(A_THREADS) k_permute(Bufs B) {
             cls[q] = valid ? (smeta[j] >> 8) : 0u;
             delta[q] = 0;
         }
-        for (int i = 0; i < g.k; ++i) {
-            int fw[2][A_ITEMS], bw[2][A_ITEMS];
+        for (int g0 = 0; g0 < ntau; g0 += TAUV) {
+            const int na = min(TAUV, ntau - g0);
+            int fw[TAUV], bw[TAUV];
 #pragma unroll
-            for (int sel = 0; sel < 2; ++sel) {
-                const int tau = 2 * i + sel;
-                const int thr = tau_value(g, tau);
-                int run = -1;
+            for (int c = 0; c < TAUV; ++c) {
+                fw[c] = -1;
+                bw[c] = 0x7fffffff;
+                if (c < na) {
+                    const int thr = tau_value(g, g0 + c);
 #pragma unroll
-                for (int q = 0; q < A_ITEMS; ++q) { if (h[q] >= thr) run = off + j0 + q; fw[sel][q] = run; }
-                int tot;
-                int cf = block_excl_scan<A_THREADS>(run, -1, OpMax(), sscan, &tot);
-                cf = max(cf, B.fwdA[(long long)t * TAU_MAX + tau]);
-#pragma unroll
-                for (int q = 0; q < A_ITEMS; ++q) fw[sel][q] = max(fw[sel][q], cf);
-                int runb = 0x7fffffff;
-#pragma unroll
-                for (int q = A_ITEMS - 1; q >= 0; --q) { bw[sel][q] = runb; if (h[q] >= thr) runb = off + j0 + q; }
-                int cb = block_excl_suffix<A_THREADS>(runb, 0x7fffffff, OpMin(), sscan);
-                cb = min(cb, B.bwdA[(long long)t * TAU_MAX + tau]);
-#pragma unroll
-                for (int q = 0; q < A_ITEMS; ++q) bw[sel][q] = min(bw[sel][q], cb);
+                    for (int q = 0; q < A_ITEMS; ++q)
+                        if (h[q] >= thr) { fw[c] = off + j0 + q; bw[c] = min(bw[c], off + j0 + q); }
+                }
             }
+            block_excl_scan_vec<A_THREADS, TAUV>(fw, -1, OpMax(), sscan, na);
+            block_excl_suffix_vec<A_THREADS, TAUV>(bw, 0x7fffffff, OpMin(), sscan, na);
 #pragma unroll
-            for (int q = 0; q < A_ITEMS; ++q) {
-                if ((cls[q] >> i) & 1u) delta[q] -= fw[0][q] - fw[1][q];
-                else delta[q] += bw[1][q] - bw[0][q];
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    fw[c] = max(fw[c], B.fwdA[(long long)t * TAU_MAX + g0 + c]);
+                    bw[c] = min(bw[c], B.bwdA[(long long)t * TAU_MAX + g0 + c]);
+                }
+            }
+            // each mask level's two thresholds (b and b+1) lie in the same group
+#pragma unroll
+            for (int c = 0; c < TAUV; c += 2) {
+                if (c + 1 >= na) continue;
+                const int i = (g0 + c) >> 1;
+                const int thr_ge = tau_value(g, g0 + c), thr_gt = tau_value(g, g0 + c + 1);
+                int last_ge = fw[c], last_gt = fw[c + 1];
+                int nxt_ge[A_ITEMS], nxt_gt[A_ITEMS];
+                int run_ge = bw[c], run_gt = bw[c + 1];
+#pragma unroll
+                for (int q = A_ITEMS - 1; q >= 0; --q) {
+                    nxt_ge[q] = run_ge;
+                    nxt_gt[q] = run_gt;
+                    if (h[q] >= thr_ge) run_ge = off + j0 + q;
+                    if (h[q] >= thr_gt) run_gt = off + j0 + q;
+                }
+#pragma unroll
+                for (int q = 0; q < A_ITEMS; ++q) {
+                    if (h[q] >= thr_ge) last_ge = off + j0 + q;
+                    if (h[q] >= thr_gt) last_gt = off + j0 + q;
+                    if ((cls[q] >> i) & 1u) delta[q] -= last_ge - last_gt;
+                    else delta[q] += nxt_gt[q] - nxt_ge[q];
+                }
             }
         }
-        const long long atot = S->a;
 #pragma unroll
         for (int q = 0; q < A_ITEMS; ++q) {
             const int j = j0 + q;
@@ -395,50 +431,87 @@ __device__ __forceinline__ long long v_count(const DevState *S) {
 }
 
 // ---------------------------------------------------------------- P partition
+// Merge-path split of (live, appended) at every multiple of B_D, one warp per
+// split: a 33-ary search (each round the 32 lanes probe 32 interior points of
+// the current range), so a split costs ~log_33(n) rounds of two dependent loads
+// (src[k], then the live key) instead of log_2(n).
+constexpr int P_THREADS = 256;
+
 template <int NW, int MODE>
-__global__ void k_partition(Bufs B) {
+__global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
     DevState *S = B.S;
     if (S->err) return;
     if (MODE == 0 && S->rot >= S->rot_end) return;
-    GenRec g;
-    if constexpr (MODE == 0) g = B.gens[S->rot];
+    __shared__ GenRec gs;
+    if constexpr (MODE == 0) {
+        if (threadIdx.x == 0) gs = B.gens[S->rot];
+        __syncthreads();
+    }
+    const GenRec &g = gs;
     const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
     const int cur = S->cur;
     const u64 *Z = B.z[cur], *X = B.x[cur];
     const long long nsplit = max(1ll, (tot + B_D - 1) / B_D);
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s <= nsplit; s += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    // pred(i): live[i] precedes appended[d-i-1] in merged order (live first on ties)
+    auto pred = [&](long long d, long long i) {
+        return !key_lt<NW>(v_key<NW, MODE>(B, g, Z, X, d - i - 1), load_key<NW>(Z, X, i));
+    };
+    for (long long s = warp0; s <= nsplit; s += nwarps) {
         const long long d = min(s * (long long)B_D, tot);
         long long lo = max(0ll, d - a), hi = min(d, n);
-        while (lo < hi) {
-            const long long mid = (lo + hi) >> 1;
-            const Key<NW> lm = load_key<NW>(Z, X, mid);
-            const Key<NW> vm = v_key<NW, MODE>(B, g, Z, X, d - mid - 1);
-            if (!key_lt<NW>(vm, lm)) lo = mid + 1; else hi = mid;
-        }
-        long long i = lo, j = d - lo;
-        // keep an equal-key run (live element followed by its appends) in one tile
-        if (j < a && (i > 0 || j > 0)) {
-            Key<NW> last;
-            if (j > 0 && i > 0) {
-                const Key<NW> lv = load_key<NW>(Z, X, i - 1);
-                const Key<NW> vv = v_key<NW, MODE>(B, g, Z, X, j - 1);
-                last = key_lt<NW>(vv, lv) ? lv : vv;
-            } else if (j > 0) {
-                last = v_key<NW, MODE>(B, g, Z, X, j - 1);
+        while (hi - lo > 32) {
+            const long long span = hi - lo;
+            const long long p = lo + (span * (lane + 1)) / 33;
+            const bool f = !pred(d, p);
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (m == 0) {
+                lo = __shfl_sync(0xffffffffu, p, 31) + 1;
             } else {
-                last = load_key<NW>(Z, X, i - 1);
+                const int fl = __ffs(m) - 1;
+                const long long pf = __shfl_sync(0xffffffffu, p, fl);
+                const long long pprev = __shfl_sync(0xffffffffu, p, fl > 0 ? fl - 1 : 0);
+                hi = pf;
+                if (fl > 0) lo = pprev + 1;
             }
-            while (j < a && key_eq<NW>(v_key<NW, MODE>(B, g, Z, X, j), last)) ++j;
         }
-        B.split_i[s] = (int)i;
-        B.split_j[s] = (int)j;
+        {
+            const long long p = lo + lane;
+            const bool f = p < hi && !pred(d, p);
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            lo = m ? lo + (__ffs(m) - 1) : hi;
+        }
+        if (lane == 0) {
+            long long i = lo, j = d - lo;
+            // keep an equal-key run (live element followed by its appends) in one tile
+            if (j < a && (i > 0 || j > 0)) {
+                Key<NW> last;
+                if (j > 0 && i > 0) {
+                    const Key<NW> lv = load_key<NW>(Z, X, i - 1);
+                    const Key<NW> vv = v_key<NW, MODE>(B, g, Z, X, j - 1);
+                    last = key_lt<NW>(vv, lv) ? lv : vv;
+                } else if (j > 0) {
+                    last = v_key<NW, MODE>(B, g, Z, X, j - 1);
+                } else {
+                    last = load_key<NW>(Z, X, i - 1);
+                }
+                while (j < a && key_eq<NW>(v_key<NW, MODE>(B, g, Z, X, j), last)) ++j;
+            }
+            B.split_i[s] = (int)i;
+            B.split_j[s] = (int)j;
+        }
     }
 }
 
 // ---------------------------------------------------------------- B merge
+constexpr int B_VPT = B_CAP / B_THREADS;   // staged inputs per thread (10)
+constexpr int B_HALF = B_VPT / 2;          // loads are issued in two batches of 5
+
 template <int NW>
 constexpr size_t merge_smem_bytes() {
-    return (size_t)B_CAP * (2 * NW * 8 + 8 + 8 + 2 + 2 + 1) + 64;
+    return (size_t)B_CAP * (2 * NW * 8 + 8 + 2 + 1) + 64;
 }
 
 // MODE 2 (clip family) filters with DevParams::clip; evolve modes with ::strict.
@@ -448,25 +521,24 @@ __device__ __forceinline__ const DevFilter &merge_filter(const DevParams &P) {
 }
 
 template <int NW, int MODE>
-__global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
+__global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
     DevState *S = B.S;
     if (S->err) return;
     if (MODE == 0 && S->rot >= S->rot_end) return;
     __shared__ GenRec g;
-    __shared__ int s_tile;
+    __shared__ int s_next[2];
     __shared__ int s_sc[B_THREADS / 32 + 1];
     __shared__ double s_red[3][B_THREADS / 32];
     __shared__ unsigned s_base;
     extern __shared__ u64 sm[];
     u64 *skz = sm;                                                    // [NW][B_CAP]
     u64 *skx = skz + NW * B_CAP;                                      // [NW][B_CAP]
-    double *sval = reinterpret_cast<double *>(skx + NW * B_CAP);      // [B_CAP] merge inputs
-    double *sout = sval + B_CAP;                                      // [B_CAP] compacted outputs
-    unsigned short *sperm = reinterpret_cast<unsigned short *>(sout + B_CAP);  // [B_CAP]
-    unsigned short *sslot = sperm + B_CAP;                            // [B_CAP]
-    unsigned char *sdead = reinterpret_cast<unsigned char *>(sslot + B_CAP);   // [B_CAP]
+    double *sval = reinterpret_cast<double *>(skx + NW * B_CAP);      // [B_CAP] inputs, then outputs
+    unsigned short *sperm = reinterpret_cast<unsigned short *>(sval + B_CAP);  // [B_CAP] merge order, then output slots
+    unsigned char *sdead = reinterpret_cast<unsigned char *>(sperm + B_CAP);   // [B_CAP]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (MODE == 0 && tid == 0) g = B.gens[S->rot];
+    if (tid == 0) s_next[0] = atomicAdd(&S->b_tile_ctr, 1);
     __syncthreads();
     const DevParams &P = *B.P;
     const DevFilter &F = merge_filter<MODE>(P);
@@ -492,54 +564,78 @@ __global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
         return k;
     };
 
-    while (true) {
-        if (tid == 0) s_tile = atomicAdd(&S->b_tile_ctr, 1);
-        __syncthreads();
-        const int t = s_tile;
-        if (t >= nsplit) break;
+    int it = 0;
+    int t = s_next[0];
+    while (t < nsplit) {
+        if (tid == 0) s_next[(it + 1) & 1] = atomicAdd(&S->b_tile_ctr, 1);  // prefetch the next tile
         const int i0 = B.split_i[t], j0 = B.split_j[t];
         const int i1 = B.split_i[t + 1], j1 = B.split_j[t + 1];
         int nl = i1 - i0, nv = j1 - j0;
         const bool bad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
         if (bad) { nl = 0; nv = 0; }
         const int ntot = nl + nv;
-        // ---- stage the live part (cos branch / early-merge pre-filter) and the appended part
+        // ---- stage the tile: every global load of a batch is issued before its
+        // shared stores (live part: cos branch / early-merge pre-filter; appended
+        // part: the sin branch of live[src[k]], computed on the fly)
         int nalive = 0;
-        for (int e = tid; e < nl; e += B_THREADS) {
-            const Key<NW> k = load_key<NW>(Z, X, i0 + e);
-            double c = C[i0 + e];
-            unsigned char dead = 0;
-            if constexpr (MODE == 0) {
-                Key<NW> q;
-                double sg;
-                const bool anti = rotate_term<NW>(k, g, &q, &sg);
-                if (pref && should_drop<NW>(P.strict, k, fabs(c))) dead = 1;
-                else if (anti) c = __dmul_rn(c, g.cosv);
-                nalive += dead ? 0 : 1;
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb) {
+            int srcp[B_HALF];
+            Key<NW> kk[B_HALF];
+            double cc[B_HALF];
+#pragma unroll
+            for (int q = 0; q < B_HALF; ++q) {
+                const int e = tid + (hb * B_HALF + q) * B_THREADS;
+                srcp[q] = 0;
+                if constexpr (MODE == 0) {
+                    if (e >= nl && e < ntot) {
+                        int p = B.src[j0 + e - nl];
+                        if (p < 0 || p >= n) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
+                        srcp[q] = p;
+                    }
+                }
             }
 #pragma unroll
-            for (int w = 0; w < NW; ++w) { skz[w * B_CAP + e] = k.z[w]; skx[w * B_CAP + e] = k.x[w]; }
-            sval[e] = c;
-            sdead[e] = dead;
-        }
-        for (int e = tid; e < nv; e += B_THREADS) {
-            Key<NW> k;
-            double c;
-            if constexpr (MODE == 0) {
-                int p = B.src[j0 + e];
-                if (p < 0 || p >= n) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
-                const Key<NW> pk = load_key<NW>(Z, X, p);
-                double sg = 0.0;
-                rotate_term<NW>(pk, g, &k, &sg);
-                c = __dmul_rn(sg * g.sinv, C[p]);
-            } else {
-                k = load_key<NW>(B.vz, B.vx, j0 + e);
-                c = B.vc[j0 + e];
+            for (int q = 0; q < B_HALF; ++q) {
+                const int e = tid + (hb * B_HALF + q) * B_THREADS;
+                if (e < nl) {
+                    kk[q] = load_key<NW>(Z, X, i0 + e);
+                    cc[q] = C[i0 + e];
+                } else if (e < ntot) {
+                    if constexpr (MODE == 0) {
+                        kk[q] = load_key<NW>(Z, X, srcp[q]);
+                        cc[q] = C[srcp[q]];
+                    } else {
+                        kk[q] = load_key<NW>(B.vz, B.vx, j0 + e - nl);
+                        cc[q] = B.vc[j0 + e - nl];
+                    }
+                }
             }
 #pragma unroll
-            for (int w = 0; w < NW; ++w) { skz[w * B_CAP + nl + e] = k.z[w]; skx[w * B_CAP + nl + e] = k.x[w]; }
-            sval[nl + e] = c;
-            sdead[nl + e] = 0;
+            for (int q = 0; q < B_HALF; ++q) {
+                const int e = tid + (hb * B_HALF + q) * B_THREADS;
+                if (e >= ntot) continue;
+                Key<NW> k = kk[q];
+                double c = cc[q];
+                unsigned char dead = 0;
+                if constexpr (MODE == 0) {
+                    Key<NW> qk;
+                    double sg = 0.0;
+                    const bool anti = rotate_term<NW>(k, g, &qk, &sg);
+                    if (e < nl) {
+                        if (pref && should_drop<NW>(P.strict, k, fabs(c))) dead = 1;
+                        else if (anti) c = __dmul_rn(c, g.cosv);
+                        nalive += dead ? 0 : 1;
+                    } else {
+                        k = qk;
+                        c = __dmul_rn(sg * g.sinv, c);
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < NW; ++w) { skz[w * B_CAP + e] = k.z[w]; skx[w * B_CAP + e] = k.x[w]; }
+                sval[e] = c;
+                sdead[e] = dead;
+            }
         }
         __syncthreads();
         // ---- merge path inside the tile; each thread owns a contiguous output range
@@ -565,11 +661,11 @@ __global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
         // ---- reduce equal-key runs (live value first, then appends in order,
         // spv_kernels.jl:338-350), strict filter on the unscaled sum, channel epilogue
         int kept = 0;
-        double outv[B_IPTMAX];
-        unsigned short slotv[B_IPTMAX];
+        double outv[B_VPT];
+        unsigned short slotv[B_VPT];
         Neu e_keep{0.0, 0.0}, e_drop{0.0, 0.0}, e_pre{0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < B_IPTMAX; ++q) {
+        for (int q = 0; q < B_VPT; ++q) {
             const int p = d0 + q;
             if (p >= dend) break;
             const int sl = sperm[p];
@@ -598,13 +694,14 @@ __global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
             ++kept;
         }
         int tkept;
-        const int loff = block_excl_scan<B_THREADS>(kept, 0, OpSum(), s_sc, &tkept);
+        const int loff = block_excl_scan<B_THREADS>(kept, 0, OpSum(), s_sc, &tkept);  // ends with a barrier
         if (warp == 0) {
             const unsigned ex = lookback_warp(B.tstat, t, epoch, (unsigned)tkept, &S->err);
             if (lane == 0) s_base = ex;
         }
+        // outputs reuse the staging buffers (every read of sval / sperm is done)
 #pragma unroll
-        for (int q = 0; q < B_IPTMAX; ++q) if (q < kept) { sout[loff + q] = outv[q]; sslot[loff + q] = slotv[q]; }
+        for (int q = 0; q < B_VPT; ++q) if (q < kept) { sval[loff + q] = outv[q]; sperm[loff + q] = slotv[q]; }
         __syncthreads();
         const long long obase = s_base;
         if (obase + tkept > B.cap) {
@@ -612,8 +709,8 @@ __global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
             tkept = 0;
         }
         for (int e = tid; e < tkept; e += B_THREADS) {
-            store_key<NW>(OZ, OX, obase + e, skey(sslot[e]));
-            OC[obase + e] = sout[e];
+            store_key<NW>(OZ, OX, obase + e, skey(sperm[e]));
+            OC[obase + e] = sval[e];
         }
         if (bad && tid == 0) atomicOr(&S->err, ERR_TILE);
         if (MODE == 0 && pref) {
@@ -639,6 +736,8 @@ __global__ void __launch_bounds__(B_THREADS) k_merge(Bufs B, int argflags) {
             }
         }
         __syncthreads();
+        ++it;
+        t = s_next[it & 1];
     }
 }
 
