@@ -80,6 +80,10 @@ struct pp_spv {
     long long bytes = 0;
     long long acap_logical_init = 16;
     long long buf_gen = 0;                 // bumped by every (re)allocation
+    int *seg_off = nullptr, *kcnt = nullptr;  // gapped window-1 merge output: segment table, tile counts
+    long long *rec = nullptr;             // per-rotation counters (window-1 WindowCounters)
+    long long rec_cap = 0;
+    bool rec_on = false;
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
     long long gexec_gen[3] = {-1, -1, -1};
 };
@@ -112,6 +116,9 @@ static Bufs make_bufs(pp_spv *h) {
     B.acap = h->acap_phys;
     B.vz = h->az; B.vx = h->ax; B.vc = h->ac;
     B.gstat = h->gstat;
+    B.rec = h->rec_on ? h->rec : nullptr;
+    B.seg_off = h->seg_off;
+    B.kcnt = h->kcnt;
     B.S = h->S; B.P = h->P; B.gens = h->gens;
     return B;
 }
@@ -147,6 +154,23 @@ static int alloc_merge_ws(pp_spv *h) {
     return PP_OK;
 }
 
+static int sync_check(pp_spv *h);
+
+// Makes the live set dense (set cur) if the last window-1 merge left it as
+// per-tile segments.
+static int ensure_dense(pp_spv *h) {
+    if (!h->seg_off) return PP_OK;
+    Bufs B;
+    memset(&B, 0, sizeof B);
+    for (int s = 0; s < 2; ++s) { B.z[s] = h->z[s]; B.x[s] = h->x[s]; B.c[s] = h->c[s]; }
+    B.S = h->S;
+    B.seg_off = h->seg_off;
+    if (h->NW == 1) k_densify<1><<<h->nsm * 4, 256, 0, h->stream>>>(B);
+    else k_densify<2><<<h->nsm * 4, 256, 0, h->stream>>>(B);
+    k_densify_commit<<<1, 32, 0, h->stream>>>(B);
+    return sync_check(h);
+}
+
 // Allocates live sets and structured-path workspaces for capacity newcap,
 // preserving the live terms (copied into set 0).
 static int grow_live(pp_spv *h, long long need) {
@@ -155,7 +179,10 @@ static int grow_live(pp_spv *h, long long need) {
     if (need > 0x7fffffffll - 8192) return fail(PP_OUT_OF_MEMORY, "term count exceeds 2^31 - 8192");
     DevState st;
     bool have = h->cap > 0;
-    if (have) TRY(read_state(h, &st));
+    if (have) {
+        TRY(ensure_dense(h));
+        TRY(read_state(h, &st));
+    }
     u64 *nz = nullptr, *nx = nullptr;
     double *nc = nullptr;
     long long saved = h->bytes;
@@ -177,10 +204,12 @@ static int grow_live(pp_spv *h, long long need) {
     TRY(dalloc(h, &h->z[1], newcap * h->NW));
     TRY(dalloc(h, &h->x[1], newcap * h->NW));
     TRY(dalloc(h, &h->c[1], newcap));
-    TRY(dalloc(h, &h->srcidx, newcap));
-    TRY(dalloc(h, &h->meta, newcap));
-    TRY(dalloc(h, &h->src, newcap));
-    long long ta = newcap / A_TILE + 2;
+    TRY(dalloc(h, &h->srcidx, newcap + SEG));
+    TRY(dalloc(h, &h->meta, newcap + SEG));
+    TRY(dalloc(h, &h->src, newcap + SEG));
+    long long ta = newcap / A_TILE + 4;
+    TRY(dalloc(h, &h->seg_off, ta + 1));
+    TRY(dalloc(h, &h->kcnt, ta));
     TRY(dalloc(h, &h->aggA, ta));
     TRY(dalloc(h, &h->offA, ta));
     TRY(dalloc(h, &h->hfirstA, ta));
@@ -238,6 +267,7 @@ static int check_err(pp_spv *h, const DevState &st) {
 }
 
 static int sync_check(pp_spv *h) {
+    if (!h->stream) return PP_OK;
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, std::string("kernel failure: ") + cudaGetErrorString(e));
     e = cudaGetLastError();
@@ -512,7 +542,7 @@ extern "C" int pp_destroy(pp_spv *h) {
     void *ptrs[] = {h->z[0], h->z[1], h->x[0], h->x[1], h->c[0], h->c[1], h->srcidx, h->src, h->meta, h->aggA,
                     h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
-                    h->S, h->P, h->gens};
+                    h->S, h->P, h->gens, h->rec, h->seg_off, h->kcnt};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
@@ -528,7 +558,7 @@ extern "C" int pp_upload(pp_spv *h, const void *z, const void *x, const double *
     if (n > 0 && (!z || !x || !c)) return fail(PP_ARGUMENT_ERROR, "null term arrays");
     DevState st;
     TRY(read_state(h, &st));
-    st.n = 0; st.an = 0; st.cur = 0; st.err = 0;
+    st.n = 0; st.an = 0; st.cur = 0; st.err = 0; st.gapped = 0;
     TRY(write_state(h, &st));
     TRY(ensure_live(h, n));
     const size_t wb = (size_t)h->NW * 8;
@@ -706,16 +736,16 @@ static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
         if (st.err & ERR_OVERFLOW) {
             st.err &= ~ERR_OVERFLOW;
             TRY(write_state(h, &st));
-            TRY(ensure_live(h, std::max(st.need + st.need / 2, 2 * st.n)));
+            TRY(ensure_live(h, std::max(st.need + st.need / 2, 3 * st.n)));
             done = st.rot;
             continue;
         }
-        TRY(check_err(h, st));
+        if (st.err) { ensure_dense(h); return check_err(h, st); }
         done = st.rot;
-        // grow ahead of time when the live set approaches capacity
-        if (done < L && 2 * st.n > h->cap) TRY(ensure_live(h, 4 * st.n));
+        // grow ahead of time: the gapped merge output needs ~1.25 (n + a) <= 2.5 n slots
+        if (done < L && 3 * st.n > h->cap) TRY(ensure_live(h, 6 * st.n));
     }
-    return PP_OK;
+    return ensure_dense(h);
 }
 
 // General path boundary: sort pending appends, merge (MODE 1).
@@ -888,9 +918,25 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     RunProf prof;
     prof.on = O.profile != 0;
     if (O.window == 1 && all_struct) {
-        TRY(ensure_live(h, 2 * st.n + 16));
+        TRY(ensure_live(h, 3 * st.n + 2 * SEG));
+        const bool want_rec = ctr && ctr->nwin > 0;
+        if (want_rec && L > h->rec_cap) {
+            TRY(dalloc(h, &h->rec, 4 * L));
+            h->rec_cap = L;
+        }
+        if (want_rec != h->rec_on) { h->rec_on = want_rec; h->buf_gen++; }
         if (h->NW == 1) TRY(run_struct<1>(h, L, ctr, &prof));
         else TRY(run_struct<2>(h, L, ctr, &prof));
+        if (want_rec) {
+            std::vector<long long> rec((size_t)(4 * L));
+            CU(cudaMemcpy(rec.data(), h->rec, 4 * L * sizeof(long long), cudaMemcpyDeviceToHost));
+            for (long long r = 0; r < L && r < ctr->nwin; ++r) {
+                if (ctr->terms_created) ctr->terms_created[r] += rec[4 * r];
+                if (ctr->merge_in) ctr->merge_in[r] += rec[4 * r + 1];
+                if (ctr->merge_out) ctr->merge_out[r] += rec[4 * r + 2];
+                if (ctr->early_merges) ctr->early_merges[r] += rec[4 * r + 3];
+            }
+        }
     } else {
         if (h->NW == 1) TRY(run_general<1>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
         else TRY(run_general<2>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
@@ -1006,6 +1052,17 @@ extern "C" int pp_stream(pp_spv *h, void **stream) {
     *stream = (void *)h->stream;
     return PP_OK;
 }
+
+#ifdef PP_PHASE_TIMERS
+extern "C" int pp_debug_phase_cycles(unsigned long long *out, int reset) {
+    cudaMemcpyFromSymbol(out, pp_phase_cycles, sizeof(unsigned long long) * 8);
+    if (reset) {
+        unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        cudaMemcpyToSymbol(pp_phase_cycles, z, sizeof z);
+    }
+    return PP_OK;
+}
+#endif
 
 extern "C" int pp_device_bytes(pp_spv *h, int64_t *bytes) {
     if (!h || !bytes) return fail(PP_ARGUMENT_ERROR, "null argument");

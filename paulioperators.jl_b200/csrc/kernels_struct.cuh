@@ -20,6 +20,24 @@
 #pragma once
 #include "blockscan.cuh"
 
+// Optional per-phase cycle counters of the merge kernel (thread 0 of each CTA;
+// compiled only with -DPP_PHASE_TIMERS, for tuning experiments).
+#ifdef PP_PHASE_TIMERS
+__device__ unsigned long long pp_phase_cycles[8];
+#define PHASE_MARK(i)                                                              \
+    do {                                                                           \
+        if (threadIdx.x == 0) {                                                    \
+            long long now_ = clock64();                                            \
+            atomicAdd(&pp_phase_cycles[i], (unsigned long long)(now_ - ph_t_));    \
+            ph_t_ = now_;                                                          \
+        }                                                                          \
+    } while (0)
+#define PHASE_START() long long ph_t_ = clock64()
+#else
+#define PHASE_MARK(i) do {} while (0)
+#define PHASE_START() do {} while (0)
+#endif
+
 namespace pp {
 
 struct Bufs {
@@ -40,6 +58,9 @@ struct Bufs {
     u64 *az, *ax;
     double *ac;
     long long acap;
+    long long *rec;               // nullable: per-rotation counters [rot][4] (window 1)
+    int *seg_off;                 // dense start of each gapped merge-output segment [nseg + 1]
+    int *kcnt;                    // survivors per merge tile (window-1 merge)
     u64 *vz, *vx;
     double *vc;
     u64 *gstat;
@@ -55,6 +76,10 @@ __device__ __forceinline__ int tau_value(const GenRec &g, int tau) {
 }
 
 // ---------------------------------------------------------------- A1 classify
+// Tiles are the segments of the live set: either consecutive A_TILE-term chunks
+// of a dense live set (set cur), or the previous window-1 merge's per-tile
+// outputs (gapped layout in set cur^1, S->gapped == 1), which this kernel also
+// compacts into the dense set cur while it classifies them.
 template <int NW>
 __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
     DevState *S = B.S;
@@ -75,16 +100,21 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
     const DevParams &P = *B.P;
     const long long n = S->n;
     const int cur = S->cur;
+    const bool gap = S->gapped != 0;
     const bool pref = n > S->acap_logical;
     const bool local_on = P.local_active != 0;
-    const u64 *Z = B.z[cur], *X = B.x[cur];
-    const double *C = B.c[cur];
-    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    u64 *Zd = B.z[cur], *Xd = B.x[cur];
+    double *Cd = B.c[cur];
+    const u64 *Zs = gap ? B.z[cur ^ 1] : Zd, *Xs = gap ? B.x[cur ^ 1] : Xd;
+    const double *Cs = gap ? B.c[cur ^ 1] : Cd;
+    const int ntiles = gap ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
     const int ntau = 2 * g.k;
+    const bool need_c = gap || pref || local_on;
 
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const long long base = (long long)t * A_TILE;
-        const int tcnt = (int)min((long long)A_TILE, n - base);
+        const long long pbase = (long long)t * A_TILE;                    // source slot of the tile
+        const long long dbase = gap ? (long long)B.seg_off[t] : pbase;     // dense index of its first term
+        const int tcnt = gap ? B.seg_off[t + 1] - B.seg_off[t] : (int)min((long long)A_TILE, n - pbase);
         bool emit[A_ITEMS];
         Key<NW> key[A_ITEMS];
 #pragma unroll
@@ -92,18 +122,21 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
             const int idx = it * A_THREADS + tid;
             emit[it] = false;
             if (idx < tcnt) {
-                key[it] = load_key<NW>(Z, X, base + idx);
+                key[it] = load_key<NW>(Zs, Xs, pbase + idx);
+                double c = 0.0;
+                if (need_c) c = Cs[pbase + idx];
+                if (gap) {
+                    store_key<NW>(Zd, Xd, dbase + idx, key[it]);
+                    Cd[dbase + idx] = c;
+                }
                 Key<NW> q;
                 double sg;
                 if (rotate_term<NW>(key[it], g, &q, &sg)) {
                     bool ok = true;
-                    if (pref || local_on) {
-                        const double c = C[base + idx];
-                        if (pref && should_drop<NW>(P.strict, key[it], fabs(c))) ok = false;
-                        if (ok && local_on) {
-                            const double cn = __dmul_rn(sg * g.sinv, c);
-                            if (should_drop<NW>(P.local, q, fabs(cn))) ok = false;
-                        }
+                    if (pref && should_drop<NW>(P.strict, key[it], fabs(c))) ok = false;
+                    if (ok && local_on) {
+                        const double cn = __dmul_rn(sg * g.sinv, c);
+                        if (should_drop<NW>(P.local, q, fabs(cn))) ok = false;
                     }
                     emit[it] = ok;
                 }
@@ -118,15 +151,25 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
         }
         __syncthreads();
         if (warp == 0) {
-            constexpr int NE = A_ITEMS * (A_THREADS / 32);  // 128 entries, 4 per lane
-            int v[NE / 32];
+            // exclusive scan of the A_ITEMS x NWARPS row-major warp counts
+            constexpr int NE = A_ITEMS * (A_THREADS / 32);
+            constexpr int PER = (NE + 31) / 32;
+            int v[PER];
             int s = 0;
 #pragma unroll
-            for (int q = 0; q < NE / 32; ++q) { v[q] = wtot[lane * (NE / 32) + q]; s += v[q]; }
+            for (int q = 0; q < PER; ++q) {
+                const int e = lane * PER + q;
+                v[q] = e < NE ? wtot[e] : 0;
+                s += v[q];
+            }
             int incl = warp_incl_scan(s, OpSum());
             int ex = incl - s;
 #pragma unroll
-            for (int q = 0; q < NE / 32; ++q) { wtot[lane * (NE / 32) + q] = ex; ex += v[q]; }
+            for (int q = 0; q < PER; ++q) {
+                const int e = lane * PER + q;
+                if (e < NE) wtot[e] = ex;
+                ex += v[q];
+            }
             if (lane == 31) s_total = incl;
         }
         if (tid < TAU_MAX) { s_first[tid] = 0x7fff; s_last[tid] = -1; }
@@ -138,7 +181,7 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
                 const int j = wtot[it * (A_THREADS / 32) + warp] + lpre[it];
 #pragma unroll
                 for (int w = 0; w < NW; ++w) { skz[w * A_TILE + j] = key[it].z[w]; skx[w * A_TILE + j] = key[it].x[w]; }
-                B.srcidx[base + j] = (int)(base + it * A_THREADS + tid);
+                B.srcidx[pbase + j] = (int)(dbase + it * A_THREADS + tid);
             }
         }
         __syncthreads();
@@ -156,7 +199,7 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
             unsigned cls = 0;
             for (int i = 0; i < g.k; ++i) cls |= (unsigned)key_bit<NW>(kj, g.level[i]) << i;
             sh[j] = (unsigned char)h;
-            B.meta[base + j] = (unsigned)h | (cls << 8);
+            B.meta[pbase + j] = (unsigned)h | (cls << 8);
         }
         __syncthreads();
         for (int tau = 0; tau < ntau; ++tau) {
@@ -219,7 +262,7 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     if (tid == 0) g = B.gens[rot];
     __syncthreads();
     const long long n = S->n;
-    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    const int ntiles = S->gapped ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
     const int tpt = (ntiles + S_THREADS - 1) / S_THREADS;
     const int t0 = min(tid * tpt, ntiles), t1 = min(t0 + tpt, ntiles);
     // tile offsets
@@ -228,8 +271,10 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     long long total;
     long long run = block_excl_scan<S_THREADS>(loc, 0ll, OpSum(), sml, &total);
     for (int t = t0; t < t1; ++t) { B.offA[t] = (int)run; run += B.aggA[t].count; }
-    if (n + total > B.cap) {
-        if (tid == 0) { S->err |= ERR_OVERFLOW; S->need = n + total; }
+    // the merge writes its tiles to fixed SEG-term slots: ceil((n + a) / B_D) of them
+    const long long slots = max(1ll, (n + total + B_D - 1) / B_D);
+    if (slots * SEG > B.cap || n + total > B.cap) {
+        if (tid == 0) { S->err |= ERR_OVERFLOW; S->need = slots * SEG + SEG; }
         return;
     }
     if (tid == 0) S->a = total;
@@ -324,7 +369,7 @@ __global__ void __launch_bounds__(A_THREADS, 2) k_permute(Bufs B) {
     __syncthreads();
     const long long n = S->n;
     const long long atot = S->a;
-    const int ntiles = (int)((n + A_TILE - 1) / A_TILE);
+    const int ntiles = S->gapped ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
     const int ntau = 2 * g.k;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int cnt = B.aggA[t].count;
@@ -507,7 +552,7 @@ __global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
 
 // ---------------------------------------------------------------- B merge
 constexpr int B_VPT = B_CAP / B_THREADS;   // staged inputs per thread (10)
-constexpr int B_HALF = B_VPT / 2;          // loads are issued in two batches of 5
+constexpr int B_HALF = B_VPT;              // loads issued in one batch per tile
 
 template <int NW>
 constexpr size_t merge_smem_bytes() {
@@ -520,8 +565,69 @@ __device__ __forceinline__ const DevFilter &merge_filter(const DevParams &P) {
     if constexpr (MODE == 2) return P.clip; else return P.strict;
 }
 
+// Filter parameters held in registers for the merge epilogue; the damped
+// exponential tables live in shared memory when a damped criterion is active.
+struct FLite {
+    long long wmax, xwmax, mwmax;
+    double thresh, dthresh_w, dthresh_xw;
+    int use_mw, use_dw, use_dxw;
+};
+
+__device__ __forceinline__ FLite flite(const DevFilter &f) {
+    FLite r;
+    r.wmax = f.wmax; r.xwmax = f.xwmax; r.mwmax = f.mwmax;
+    r.thresh = f.thresh; r.dthresh_w = f.dthresh_w; r.dthresh_xw = f.dthresh_xw;
+    r.use_mw = f.use_mw; r.use_dw = f.use_dw; r.use_dxw = f.use_dxw;
+    return r;
+}
+
+// should_drop (spv_kernels.jl:64-79) with register parameters.
+template <int NW>
+__device__ __forceinline__ bool drop_lite(const FLite &f, const double *sexpw, const double *sexpxw, const Key<NW> &k,
+                                          double absc) {
+    if (absc <= f.thresh) return true;
+    u64 o[NW];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) o[w] = k.z[w] | k.x[w];
+    const int wt = popc_w<NW>(o);
+    if (wt > f.wmax) return true;
+    const int xw = popc_w<NW>(k.x);
+    if (xw > f.xwmax) return true;
+    if (f.use_mw && majorana<NW>(k) > f.mwmax) return true;
+    if (f.use_dw && __dmul_rn(absc, sexpw[wt]) <= f.dthresh_w) return true;
+    if (f.use_dxw && __dmul_rn(absc, sexpxw[xw]) <= f.dthresh_xw) return true;
+    return false;
+}
+
+template <int NW>
+__device__ __forceinline__ double chan_lite(int kind, const u64 *mask, const double *tX, const double *tY,
+                                           const double *tZ, const Key<NW> &k) {
+    if (kind == 4) {
+        int nX = 0, nY = 0, nZ = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const u64 xM = k.x[w] & mask[w], zM = k.z[w] & mask[w];
+            nX += __popcll(xM & ~k.z[w]);
+            nY += __popcll(xM & k.z[w]);
+            nZ += __popcll(zM & ~k.x[w]);
+        }
+        return __dmul_rn(__dmul_rn(tX[nX], tY[nY]), tZ[nZ]);
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const u64 s = kind == 0 ? (k.z[w] | k.x[w]) : kind == 1 ? k.x[w] : kind == 2 ? k.z[w] : (k.x[w] ^ k.z[w]);
+        cnt += __popcll(s & mask[w]);
+    }
+    return tX[cnt];
+}
+
+// One merge tile: the merge-path diagonal range [split[t], split[t+1]) of
+// (live, appended).  Each CTA loops over tiles taken in order from a counter;
+// while warp 0 resolves the tile's output offset by decoupled look-back, the
+// other warps already issue the next tile's global loads into registers.
 template <int NW, int MODE>
-__global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
+__global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     DevState *S = B.S;
     if (S->err) return;
     if (MODE == 0 && S->rot >= S->rot_end) return;
@@ -530,6 +636,7 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
     __shared__ int s_sc[B_THREADS / 32 + 1];
     __shared__ double s_red[3][B_THREADS / 32];
     __shared__ unsigned s_base;
+    __shared__ double s_expw[130], s_expxw[130], s_ch[3][130];
     extern __shared__ u64 sm[];
     u64 *skz = sm;                                                    // [NW][B_CAP]
     u64 *skx = skz + NW * B_CAP;                                      // [NW][B_CAP]
@@ -539,13 +646,25 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (MODE == 0 && tid == 0) g = B.gens[S->rot];
     if (tid == 0) s_next[0] = atomicAdd(&S->b_tile_ctr, 1);
-    __syncthreads();
     const DevParams &P = *B.P;
     const DevFilter &F = merge_filter<MODE>(P);
+    const FLite fl = flite(F);
+    for (int i = tid; i < 130; i += B_THREADS) {
+        if (fl.use_dw) s_expw[i] = F.expw[i];
+        if (fl.use_dxw) s_expxw[i] = F.expxw[i];
+    }
+    __syncthreads();
     const int flags = MODE == 0 ? g.flags : argflags;
     const bool do_chan = MODE != 2 && (flags & GEN_CHANNEL) != 0 && P.chan_kind >= 0;
     const bool do_corr = MODE != 2 && P.corr_kind == 1;
     const bool do_meas = (flags & GEN_MEASURE) != 0 || do_corr;
+    const int chan_kind = P.chan_kind;
+    const u64 chan_mask[2] = {P.chan_mask[0], P.chan_mask[1]};
+    if (do_chan) {
+        for (int i = tid; i < 130; i += B_THREADS) { s_ch[0][i] = P.chanX[i]; s_ch[1][i] = P.chanY[i]; s_ch[2][i] = P.chanZ[i]; }
+    }
+    FLite fs;                       // early-merge pre-filter (the strict filter of the evolve call)
+    if constexpr (MODE == 0) fs = flite(P.strict);
     const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
     const int cur = S->cur;
     const u64 *Z = B.z[cur], *X = B.x[cur];
@@ -567,19 +686,20 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
     int it = 0;
     int t = s_next[0];
     while (t < nsplit) {
-        if (tid == 0) s_next[(it + 1) & 1] = atomicAdd(&S->b_tile_ctr, 1);  // prefetch the next tile
+        if (tid == 0) s_next[(it + 1) & 1] = atomicAdd(&S->b_tile_ctr, 1);  // next tile index
         const int i0 = B.split_i[t], j0 = B.split_j[t];
         const int i1 = B.split_i[t + 1], j1 = B.split_j[t + 1];
         int nl = i1 - i0, nv = j1 - j0;
-        const bool bad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
-        if (bad) { nl = 0; nv = 0; }
+        const bool tbad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
+        if (tbad) { nl = 0; nv = 0; }
         const int ntot = nl + nv;
-        // ---- stage the tile: every global load of a batch is issued before its
-        // shared stores (live part: cos branch / early-merge pre-filter; appended
-        // part: the sin branch of live[src[k]], computed on the fly)
+        PHASE_START();
+        // ---- stage the tile, two batches of loads each issued before its shared
+        // stores: the live part gets the cos branch / early-merge pre-filter, the
+        // appended part is the sin branch of live[src[k]] computed on the fly
         int nalive = 0;
 #pragma unroll
-        for (int hb = 0; hb < 2; ++hb) {
+        for (int hb = 0; hb < B_VPT / B_HALF; ++hb) {
             int srcp[B_HALF];
             Key<NW> kk[B_HALF];
             double cc[B_HALF];
@@ -623,7 +743,7 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
                     double sg = 0.0;
                     const bool anti = rotate_term<NW>(k, g, &qk, &sg);
                     if (e < nl) {
-                        if (pref && should_drop<NW>(P.strict, k, fabs(c))) dead = 1;
+                        if (pref && drop_lite<NW>(fs, F.expw, F.expxw, k, fabs(c))) dead = 1;
                         else if (anti) c = __dmul_rn(c, g.cosv);
                         nalive += dead ? 0 : 1;
                     } else {
@@ -638,6 +758,7 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
             }
         }
         __syncthreads();
+        PHASE_MARK(0);
         // ---- merge path inside the tile; each thread owns a contiguous output range
         // (live first on equal keys: spv_kernels.jl:338)
         const int ipt = (ntot + B_THREADS - 1) / B_THREADS;
@@ -658,51 +779,71 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
             }
         }
         __syncthreads();
+        PHASE_MARK(1);
         // ---- reduce equal-key runs (live value first, then appends in order,
         // spv_kernels.jl:338-350), strict filter on the unscaled sum, channel epilogue
-        int kept = 0;
-        double outv[B_VPT];
-        unsigned short slotv[B_VPT];
+        double outq[B_VPT];
+        unsigned short slotq[B_VPT];
+        unsigned keepm = 0;
         Neu e_keep{0.0, 0.0}, e_drop{0.0, 0.0}, e_pre{0.0, 0.0};
+        Key<NW> kprev;
+        if (d0 > 0 && d0 < dend) kprev = skey(sperm[d0 - 1]);
 #pragma unroll
         for (int q = 0; q < B_VPT; ++q) {
             const int p = d0 + q;
-            if (p >= dend) break;
+            outq[q] = 0.0;
+            slotq[q] = 0;
+            if (p >= dend) continue;
             const int sl = sperm[p];
             const Key<NW> kp = skey(sl);
-            if (p > 0 && key_eq<NW>(skey(sperm[p - 1]), kp)) continue;  // not a run head
+            const bool head = !(p > 0 && key_eq<NW>(kprev, kp));
+            kprev = kp;
+            if (!head) continue;
             double acc = 0.0;
             bool have = false;
             const bool diag = is_diag<NW>(kp);
             const double sgn = diag ? ket_sign<NW>(kp, ket) : 0.0;
             for (int r = p; r < ntot; ++r) {
-                const int sr = sperm[r];
+                const int sr = r == p ? sl : sperm[r];
                 if (r > p && !key_eq<NW>(skey(sr), kp)) break;
                 if (sdead[sr]) { if (diag && do_meas) e_pre.add(sgn * sval[sr]); continue; }
                 acc = have ? __dadd_rn(acc, sval[sr]) : sval[sr];
                 have = true;
             }
             if (!have) continue;
-            if (should_drop<NW>(F, kp, fabs(acc))) {
+            if (drop_lite<NW>(fl, s_expw, s_expxw, kp, fabs(acc))) {
                 if (diag && do_meas) e_drop.add(sgn * acc);
                 continue;
             }
-            const double o = do_chan ? __dmul_rn(acc, channel_factor<NW>(P, kp)) : acc;
+            const double o = do_chan ? __dmul_rn(acc, chan_lite<NW>(chan_kind, chan_mask, s_ch[0], s_ch[1], s_ch[2], kp)) : acc;
             if (diag && do_meas) e_keep.add(sgn * o);
-            outv[kept] = o;
-            slotv[kept] = (unsigned short)sl;
-            ++kept;
+            outq[q] = o;
+            slotq[q] = (unsigned short)sl;
+            keepm |= 1u << q;
         }
+        PHASE_MARK(2);
+        const int kept = __popc(keepm);
         int tkept;
         const int loff = block_excl_scan<B_THREADS>(kept, 0, OpSum(), s_sc, &tkept);  // ends with a barrier
-        if (warp == 0) {
+        PHASE_MARK(3);
+        if constexpr (MODE == 0) {
+            // window-1 merge: the tile's survivors go to its own SEG-term slot (the
+            // gapped layout that the next classify compacts), no look-back wait
+            if (tid == 0) { s_base = (unsigned)((long long)t * SEG); B.kcnt[t] = tkept; }
+        } else if (warp == 0) {
             const unsigned ex = lookback_warp(B.tstat, t, epoch, (unsigned)tkept, &S->err);
             if (lane == 0) s_base = ex;
         }
+        PHASE_MARK(4);
         // outputs reuse the staging buffers (every read of sval / sperm is done)
+        {
+            int o = loff;
 #pragma unroll
-        for (int q = 0; q < B_VPT; ++q) if (q < kept) { sval[loff + q] = outv[q]; sperm[loff + q] = slotv[q]; }
+            for (int q = 0; q < B_VPT; ++q) if ((keepm >> q) & 1u) { sval[o] = outq[q]; sperm[o] = slotq[q]; ++o; }
+        }
+        const int tn = s_next[(it + 1) & 1];
         __syncthreads();
+        PHASE_MARK(7);
         const long long obase = s_base;
         if (obase + tkept > B.cap) {
             if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
@@ -712,7 +853,8 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
             store_key<NW>(OZ, OX, obase + e, skey(sperm[e]));
             OC[obase + e] = sval[e];
         }
-        if (bad && tid == 0) atomicOr(&S->err, ERR_TILE);
+        PHASE_MARK(5);
+        if (tbad && tid == 0) atomicOr(&S->err, ERR_TILE);
         if (MODE == 0 && pref) {
             int na = nalive;
 #pragma unroll
@@ -736,8 +878,9 @@ __global__ void __launch_bounds__(B_THREADS, 3) k_merge(Bufs B, int argflags) {
             }
         }
         __syncthreads();
+        PHASE_MARK(6);
         ++it;
-        t = s_next[it & 1];
+        t = tn;
     }
 }
 
@@ -777,21 +920,52 @@ __global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
             if (do_corr) S->corr_energy = __dsub_rn(S->corr_energy, __dadd_rn(f1.s + f1.c, f2.s + f2.c));
         }
     }
+    __shared__ long long s_tot;
+    __shared__ int s_scan[256 / 32 + 1];
+    if constexpr (MODE == 0) {
+        // window-1 merge: segment table of the gapped output (dense start of each
+        // tile's survivors), scanned in tile order
+        const int per = (nsplit + 255) / 256;
+        const int t0 = min(tid * per, nsplit), t1 = min(t0 + per, nsplit);
+        int loc = 0;
+        for (int tt = t0; tt < t1; ++tt) loc += B.kcnt[tt];
+        int all;
+        int run = block_excl_scan<256>(loc, 0, OpSum(), s_scan, &all);
+        for (int tt = t0; tt < t1; ++tt) { B.seg_off[tt] = run; run += B.kcnt[tt]; }
+        if (tid == 0) { B.seg_off[nsplit] = all; s_tot = all; }
+        __syncthreads();
+    } else {
+        if (tid == 0) s_tot = (long long)(unsigned)(st_load(B.tstat + (nsplit - 1)) & 0xffffffffu);
+        __syncthreads();
+    }
     if (tid == 0) {
         const bool pref = MODE == 0 && n > S->acap_logical;
-        const u64 st = st_load(B.tstat + (nsplit - 1));
-        const long long total = (long long)(unsigned)(st & 0xffffffffu);
+        const long long total = s_tot;
         S->n = total;
-        S->cur ^= 1;
+        if (MODE == 0) {
+            S->gapped = 1;
+            S->nseg = nsplit;
+        } else {
+            S->cur ^= 1;
+        }
         S->merge_in += tot;
         S->merge_out += total;
         if (total > S->peak) S->peak = total;
         if (MODE == 0) {
             S->live_in += n;
             S->created += a;
+            const long long np = pref ? S->npref : n;
+            if (B.rec) {
+                // WindowCounters of this rotation (window = 1): an early boundary
+                // merges n -> np first, the regular one np + a -> total
+                long long *r = B.rec + 4 * S->rot;
+                r[0] = a;
+                r[1] = (pref ? n : 0) + np + a;
+                r[2] = (pref ? np : 0) + total;
+                r[3] = pref ? 1 : 0;
+            }
             if (pref) {
                 S->early += 1;
-                const long long np = S->npref;
                 if (np > S->acap_logical) S->acap_logical = max(2 * S->acap_logical, np);
                 S->npref = 0;
             }
@@ -801,6 +975,33 @@ __global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
         S->b_tile_ctr = 0;
         S->epoch += 1;
     }
+}
+
+// Compacts a gapped window-1 merge output (set cur^1, segment table seg_off)
+// into the dense set cur; k_densify_commit then marks the state dense.
+template <int NW>
+__global__ void k_densify(Bufs B) {
+    DevState *S = B.S;
+    if (!S->gapped) return;
+    const int cur = S->cur;
+    const int nseg = (int)S->nseg;
+    const u64 *Zs = B.z[cur ^ 1], *Xs = B.x[cur ^ 1];
+    const double *Cs = B.c[cur ^ 1];
+    u64 *Zd = B.z[cur], *Xd = B.x[cur];
+    double *Cd = B.c[cur];
+    for (int t = blockIdx.x; t < nseg; t += gridDim.x) {
+        const long long d0 = B.seg_off[t];
+        const int cnt = B.seg_off[t + 1] - B.seg_off[t];
+        const long long p0 = (long long)t * SEG;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            store_key<NW>(Zd, Xd, d0 + e, load_key<NW>(Zs, Xs, p0 + e));
+            Cd[d0 + e] = Cs[p0 + e];
+        }
+    }
+}
+
+__global__ void k_densify_commit(Bufs B) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) B.S->gapped = 0;
 }
 
 }  // namespace pp

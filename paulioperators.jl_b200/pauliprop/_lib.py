@@ -11,7 +11,7 @@ import os
 from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_void_p
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpauliprop.so")
+LIB_PATH = os.environ.get("PAULIPROP_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libpauliprop.so")
 
 PP_OK = 0
 PP_ARGUMENT_ERROR = 1

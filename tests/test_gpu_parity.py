@@ -386,3 +386,28 @@ def test_copy_and_nonmutating():
     assert g.to_paulisum() == before
     v.evolve1(3, 5, 0.4)
     compare(g2, v, bitexact=True)
+
+
+def test_window1_counters_match_oracle():
+    """WindowCounters at window 1 (one window per rotation), including the early
+    boundaries forced by the append capacity (spv_evolve.jl:356-383)."""
+    rng = random.Random(11)
+    N = 10
+    terms = rand_terms(rng, N, 300)
+    for k in list(terms)[:60]:
+        terms[k] = 1e-9
+    gens = [((1 << 1) | (1 << 2), 0), (0, 1 << 4), ((1 << 3) | (1 << 7), 0), (1 << 5, 1 << 5)] * 5
+    angs = [0.4, 0.3, -0.7, 0.9] * 5
+    spec = ("comp", [("coeff", 1e-6), ("weight", 6)])
+    v = oracle_from_terms(N, terms, append_factor=0.2, min_capacity=4)
+    g = gpu_from_oracle(v, N, append_cap=v.append_cap)
+    _, ctr = v.evolve(gens, angs, window=1, strict=filt(spec), nwin=len(gens))
+    wc = pp.WindowCounters(len(gens))
+    pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs, truncation=strategy(spec), counters=wc)
+    assert ctr[3].sum() > 0
+    assert np.array_equal(wc.terms_created, ctr[0])
+    assert np.array_equal(wc.merge_in, ctr[1])
+    assert np.array_equal(wc.merge_out, ctr[2])
+    assert np.array_equal(wc.early_merges, ctr[3])
+    assert np.all(wc.t_rotate > 0) and np.all(wc.t_merge > 0)
+    compare(g, v, bitexact=True)
