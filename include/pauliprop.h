@@ -124,6 +124,23 @@ int pp_evolve(pp_spv *h, const void *gz, const void *gx, const double *cosv, con
  * weight_damped_clip! / x_weight_damped_clip! and the compilable truncate!
  * (spv_evolve.jl:13-26, 59-65) -> _compact_spv! (spv_kernels.jl:395-408). */
 int pp_compact(pp_spv *h, const pp_filter *f);
+/* Largest term count pp_compact_static accepts: the size its static scratch covers. */
+#define PP_COMPACT_STATIC_MAX_TERMS (1 << 25)
+/* No counterpart in the reference.  The clip / compaction of pp_compact for a
+ * caller that cannot allocate device memory — one whose device memory is owned by
+ * another allocator, or that calls from a phase where allocating is not allowed —
+ * and so cannot hold a pp_spv handle.  Reads n terms (z, x, c: device arrays in
+ * the word layout above), writes the terms that filter f keeps, in order, to
+ * z_out / x_out / c_out (device arrays with room for n terms), and stores their
+ * count in *n_out (host).  Allocates nothing: its look-back scratch is a static
+ * device array of 8 + PP_COMPACT_STATIC_MAX_TERMS/1024 words that every GPU loading
+ * the library holds until exit.  The first call on a device looks up that array's
+ * address, so make it before any stream capture.  All calls share the scratch:
+ * calls whose work overlaps on the GPU race on it.  n > PP_COMPACT_STATIC_MAX_TERMS
+ * gives PP_ARGUMENT_ERROR.  stream: a cudaStream_t (NULL: the default stream); the
+ * call synchronizes it. */
+int pp_compact_static(int32_t N, const void *z, const void *x, const double *c, int64_t n, const pp_filter *f,
+                      void *z_out, void *x_out, double *c_out, int64_t *n_out, void *stream);
 /* _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114). */
 int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh);
 /* depolarizing_channel! (channels.jl:223-232, kind 0), dephasing_channel! (234-243, 1),

@@ -29,6 +29,7 @@ static int fail(int code, const std::string &msg) {
     return code;
 }
 extern "C" const char *pp_last_error(void) { return g_err.c_str(); }
+int pp_fail_msg(int code, const char *msg) { return fail(code, msg); }
 
 #define CU(call)                                                                         \
     do {                                                                                 \

@@ -83,6 +83,8 @@ SIGNATURES = {
     "pp_evolve1": (c_int32, [c_void_p, c_void_p, c_void_p, c_double, c_double]),
     "pp_evolve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPEvolveOpts)]),
     "pp_compact": (c_int32, [c_void_p, POINTER(PPFilter)]),
+    "pp_compact_static": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPFilter),
+                                    c_void_p, c_void_p, c_void_p, POINTER(c_int64), c_void_p]),
     "pp_adaptive": (c_int32, [c_void_p, c_int64, c_double]),
     "pp_channel": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
     "pp_expect_ket": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
