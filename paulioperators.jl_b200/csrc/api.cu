@@ -60,7 +60,7 @@ struct pp_spv {
     unsigned *meta = nullptr;
     TileAggA *aggA = nullptr;
     int *offA = nullptr, *hfirstA = nullptr, *fwdA = nullptr, *bwdA = nullptr;
-    int *split_i = nullptr, *split_j = nullptr;
+    int *split_i = nullptr, *split_j = nullptr, *split_k = nullptr;
     u64 *tstat = nullptr, *gstat = nullptr;
     double *part = nullptr;
     long long nsplit_cap = 0, gtiles_cap = 0;
@@ -81,7 +81,8 @@ struct pp_spv {
     long long bytes = 0;
     long long acap_logical_init = 16;
     long long buf_gen = 0;                 // bumped by every (re)allocation
-    int *seg_off = nullptr, *kcnt = nullptr;  // gapped window-1 merge output: segment table, tile counts
+    int *sphys = nullptr, *soff = nullptr;   // live segment table (physical base, dense start)
+    int *kcnt = nullptr;                     // survivors per window-1 merge tile
     long long *rec = nullptr;             // per-rotation counters (window-1 WindowCounters)
     long long rec_cap = 0;
     bool rec_on = false;
@@ -112,13 +113,13 @@ static Bufs make_bufs(pp_spv *h) {
     B.cap = h->cap;
     B.srcidx = h->srcidx; B.meta = h->meta; B.src = h->src;
     B.aggA = h->aggA; B.offA = h->offA; B.hfirstA = h->hfirstA; B.fwdA = h->fwdA; B.bwdA = h->bwdA;
-    B.split_i = h->split_i; B.split_j = h->split_j; B.tstat = h->tstat; B.part = h->part;
+    B.split_i = h->split_i; B.split_j = h->split_j; B.split_k = h->split_k; B.tstat = h->tstat; B.part = h->part;
     B.az = h->az; B.ax = h->ax; B.ac = h->ac;
     B.acap = h->acap_phys;
     B.vz = h->az; B.vx = h->ax; B.vc = h->ac;
     B.gstat = h->gstat;
     B.rec = h->rec_on ? h->rec : nullptr;
-    B.seg_off = h->seg_off;
+    B.sphys = h->sphys; B.soff = h->soff;
     B.kcnt = h->kcnt;
     B.S = h->S; B.P = h->P; B.gens = h->gens;
     return B;
@@ -141,6 +142,10 @@ static int alloc_merge_ws(pp_spv *h) {
     if (need > h->nsplit_cap) {
         TRY(dalloc(h, &h->split_i, need + 1));
         TRY(dalloc(h, &h->split_j, need + 1));
+        TRY(dalloc(h, &h->split_k, need + 1));
+        TRY(dalloc(h, &h->kcnt, need + 1));
+        TRY(dalloc(h, &h->sphys, need + 1));
+        TRY(dalloc(h, &h->soff, need + 1));
         TRY(dalloc(h, &h->tstat, need));
         TRY(dalloc(h, &h->part, need * 4));
         CU(cudaMemsetAsync(h->tstat, 0, need * sizeof(u64), h->stream));
@@ -157,15 +162,16 @@ static int alloc_merge_ws(pp_spv *h) {
 
 static int sync_check(pp_spv *h);
 
-// Makes the live set dense (set cur) if the last window-1 merge left it as
-// per-tile segments.
+// Makes the live set dense if the last window-1 merge left it as per-tile
+// slots (seg_dense == 0): copies it into the other set and flips the parity.
 static int ensure_dense(pp_spv *h) {
-    if (!h->seg_off) return PP_OK;
+    if (!h->soff) return PP_OK;
     Bufs B;
     memset(&B, 0, sizeof B);
     for (int s = 0; s < 2; ++s) { B.z[s] = h->z[s]; B.x[s] = h->x[s]; B.c[s] = h->c[s]; }
     B.S = h->S;
-    B.seg_off = h->seg_off;
+    B.sphys = h->sphys;
+    B.soff = h->soff;
     if (h->NW == 1) k_densify<1><<<h->nsm * 4, 256, 0, h->stream>>>(B);
     else k_densify<2><<<h->nsm * 4, 256, 0, h->stream>>>(B);
     k_densify_commit<<<1, 32, 0, h->stream>>>(B);
@@ -208,9 +214,7 @@ static int grow_live(pp_spv *h, long long need) {
     TRY(dalloc(h, &h->srcidx, newcap + SEG));
     TRY(dalloc(h, &h->meta, newcap + SEG));
     TRY(dalloc(h, &h->src, newcap + SEG));
-    long long ta = newcap / A_TILE + 4;
-    TRY(dalloc(h, &h->seg_off, ta + 1));
-    TRY(dalloc(h, &h->kcnt, ta));
+    long long ta = newcap / SEG + 4;
     TRY(dalloc(h, &h->aggA, ta));
     TRY(dalloc(h, &h->offA, ta));
     TRY(dalloc(h, &h->hfirstA, ta));
@@ -531,6 +535,7 @@ extern "C" int pp_create(int32_t N, int64_t live_cap, int64_t append_cap, pp_spv
     DevState st;
     memset(&st, 0, sizeof st);
     st.acap_logical = h->acap_logical_init;
+    st.seg_dense = 1;
     if ((r = write_state(h, &st))) return bail(r);
     if ((r = grow_live(h, std::max<int64_t>(live_cap, 4096)))) return bail(r);
     *out = h;
@@ -543,7 +548,7 @@ extern "C" int pp_destroy(pp_spv *h) {
     void *ptrs[] = {h->z[0], h->z[1], h->x[0], h->x[1], h->c[0], h->c[1], h->srcidx, h->src, h->meta, h->aggA,
                     h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
-                    h->S, h->P, h->gens, h->rec, h->seg_off, h->kcnt};
+                    h->S, h->P, h->gens, h->rec, h->sphys, h->soff, h->kcnt, h->split_k};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
@@ -559,7 +564,7 @@ extern "C" int pp_upload(pp_spv *h, const void *z, const void *x, const double *
     if (n > 0 && (!z || !x || !c)) return fail(PP_ARGUMENT_ERROR, "null term arrays");
     DevState st;
     TRY(read_state(h, &st));
-    st.n = 0; st.an = 0; st.cur = 0; st.err = 0; st.gapped = 0;
+    st.n = 0; st.an = 0; st.cur = 0; st.err = 0; st.seg_dense = 1;
     TRY(write_state(h, &st));
     TRY(ensure_live(h, n));
     const size_t wb = (size_t)h->NW * 8;
@@ -619,6 +624,7 @@ extern "C" int pp_copy(pp_spv *h, pp_spv **out) {
     memset(&so, 0, sizeof so);
     so.n = st.n;
     so.acap_logical = st.acap_logical;
+    so.seg_dense = 1;
     int r = write_state(o, &so);
     if (r) { pp_destroy(o); return r; }
     *out = o;
@@ -673,10 +679,16 @@ static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
     long long done = 0;
     const bool timed = prof->on || (ctr && (ctr->t_rotate || ctr->t_merge));
     std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
+    bool table = false;            // the device segment table describes the (dense) live set
     while (done < L) {
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
+        if (!table) {
+            k_segdense<<<h->nsm, 256, 0, s>>>(B);
+            prof->launches += 1;
+            table = true;
+        }
         if (!timed) {
             // replay captured chunks: CHUNK_ROT, then 8, then single rotations
             long long r = done;
@@ -738,13 +750,17 @@ static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
             st.err &= ~ERR_OVERFLOW;
             TRY(write_state(h, &st));
             TRY(ensure_live(h, std::max(st.need + st.need / 2, 3 * st.n)));
+            table = false;
             done = st.rot;
             continue;
         }
         if (st.err) { ensure_dense(h); return check_err(h, st); }
         done = st.rot;
-        // grow ahead of time: the gapped merge output needs ~1.25 (n + a) <= 2.5 n slots
-        if (done < L && 3 * st.n > h->cap) TRY(ensure_live(h, 6 * st.n));
+        // grow ahead of time: the merge's per-tile output slots need ~1.25 (n + a) <= 2.5 n
+        if (done < L && 3 * st.n > h->cap) {
+            TRY(ensure_live(h, 6 * st.n));
+            table = false;
+        }
     }
     return ensure_dense(h);
 }

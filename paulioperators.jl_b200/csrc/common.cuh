@@ -75,7 +75,7 @@ struct DevState {
     long long npref;              // survivors of the window-1 early-merge pre-filter
     long long live_in;            // sum of live counts entering rotations
     long long peak;               // largest live count after a merge
-    long long nseg;               // segments of the gapped merge output (gapped == 1)
+    long long nseg;               // segments of the live set's segment table
     double expect_val;            // last reduced <ket|O|ket> (after the merge)
     double corr_energy;           // EnergyCorrection.accumulated_energy (delta this call)
     int cur;                      // live buffer set (0/1)
@@ -84,7 +84,7 @@ struct DevState {
     int b_tile_ctr, b_done;       // merge kernel tile dispenser / completion
     int g_tile_ctr, g_done;       // general rotate kernel
     int measure_valid;
-    int gapped;                   // 1: live terms are the last merge's per-tile segments in set cur^1
+    int seg_dense;                // 0: live set cur is the last window-1 merge's per-tile slots (segment table)
     int pad;
 };
 
@@ -96,8 +96,8 @@ constexpr int B_THREADS = 512;
 constexpr int B_D = 2048;                     // merge-path diagonal step (outputs per tile)
 constexpr int B_IPTMAX = 5;                   // per-thread outputs at most
 constexpr int B_CAP = B_THREADS * B_IPTMAX;   // 2560: a tile plus an equal-key run past its diagonal
-constexpr int SEG = B_CAP;                    // slot of one merge tile's output in the gapped layout
-static_assert(A_TILE == SEG, "classify tiles are the merge output segments");
+constexpr int SEG = B_CAP;                    // slot of one window-1 merge tile's output; dense segment size
+static_assert(A_TILE >= SEG, "a classify tile holds one live segment");
 constexpr int G_THREADS = 256;
 constexpr int G_ITEMS = 8;
 constexpr int G_TILE = G_THREADS * G_ITEMS;   // general rotate tile

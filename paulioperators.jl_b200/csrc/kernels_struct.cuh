@@ -1,22 +1,29 @@
-// Window-1 rotation as one sort-free pass structure (the GPU counterpart of
+// Window-1 rotation as a sort-free pass structure (the GPU counterpart of
 // _rotate_range! + _gather_append! + _unshuffle_ws! + _try_merge!,
 // spv_kernels.jl:146-177, 187-193, 262-363, driven as in spv_evolve.jl:352-385).
 //
 // The sin branches of one rotation are the keys P xor M (M = (gz, gx)) of the
 // anticommuting live terms P.  Since live is sorted, the appended keys are
-// sorted by key xor M; their sorted position is the classic rank identity
+// sorted by key xor M; their sorted position is the rank identity
 //   rank(P xor M) = rank(P) + sum_{b in M} ([P_b = 0] - [P_b = 1]) * sib_b(P),
 // where sib_b(P) counts emitted terms that share P's bits above level b and
 // differ at b.  sib_b comes from the positions where the "highest differing
 // bit" h between consecutive emitted keys crosses b and b+1, i.e. from
 // forward/backward max/min scans.  Kernels:
-//   k_classify  (A1) tile-local compaction of emitting terms, h, tile aggregates
+//   k_classify  (A1) per-segment compaction of emitting terms, h, tile aggregates
 //   k_tilescan  (A2) one CTA: tile offsets and cross-tile scan carries
-//   k_permute   (A3) final ranks -> src[rank] = live index (no key traffic)
+//   k_permute   (A3) final ranks -> src[rank] = physical live index (no key traffic)
 //   k_partition (P)  merge-path split of (live, virtual sorted appends)
-//   k_merge     (B)  merge + reduce-by-key + filter + channel + compaction
+//   k_merge     (B)  merge + reduce-by-key + filter + channel epilogue
+//   k_commit         segment table of the output, counters, partial reductions
 // The appended keys are never materialised: B gathers live[src[k]] and applies
 // the xor and the phase on the fly.
+//
+// Live layout: a segment table.  Segment k (all non-empty) holds the terms of
+// dense indices [soff[k], soff[k+1]) at physical positions sphys[k] + j of the
+// live set `cur`.  A window-1 merge writes each output tile to its own SEG-term
+// slot (no cross-tile offset wait) and k_commit lists the non-empty slots; a
+// dense live set is the table with sphys[k] = soff[k] = k * SEG.
 #pragma once
 #include "blockscan.cuh"
 
@@ -51,7 +58,7 @@ struct Bufs {
     TileAggA *aggA;
     int *offA, *hfirstA, *fwdA, *bwdA;
     // merge
-    int *split_i, *split_j;
+    int *split_i, *split_j, *split_k;
     u64 *tstat;
     double *part;
     // general path (direct V = sorted appends)
@@ -59,7 +66,7 @@ struct Bufs {
     double *ac;
     long long acap;
     long long *rec;               // nullable: per-rotation counters [rot][4] (window 1)
-    int *seg_off;                 // dense start of each gapped merge-output segment [nseg + 1]
+    int *sphys, *soff;            // live segment table: physical base / dense start [nseg + 1]
     int *kcnt;                    // survivors per merge tile (window-1 merge)
     u64 *vz, *vx;
     double *vc;
@@ -76,10 +83,9 @@ __device__ __forceinline__ int tau_value(const GenRec &g, int tau) {
 }
 
 // ---------------------------------------------------------------- A1 classify
-// Tiles are the segments of the live set: either consecutive A_TILE-term chunks
-// of a dense live set (set cur), or the previous window-1 merge's per-tile
-// outputs (gapped layout in set cur^1, S->gapped == 1), which this kernel also
-// compacts into the dense set cur while it classifies them.
+// One tile per live segment: anticommutation, tile-local compaction of the terms
+// that emit a sin branch, their h levels and the tile aggregates.  srcidx holds
+// the physical index of each emitting term (used by the merge's gather).
 template <int NW>
 __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
     DevState *S = B.S;
@@ -100,21 +106,17 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
     const DevParams &P = *B.P;
     const long long n = S->n;
     const int cur = S->cur;
-    const bool gap = S->gapped != 0;
     const bool pref = n > S->acap_logical;
     const bool local_on = P.local_active != 0;
-    u64 *Zd = B.z[cur], *Xd = B.x[cur];
-    double *Cd = B.c[cur];
-    const u64 *Zs = gap ? B.z[cur ^ 1] : Zd, *Xs = gap ? B.x[cur ^ 1] : Xd;
-    const double *Cs = gap ? B.c[cur ^ 1] : Cd;
-    const int ntiles = gap ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
+    const u64 *Z = B.z[cur], *X = B.x[cur];
+    const double *C = B.c[cur];
+    const int ntiles = (int)S->nseg;
     const int ntau = 2 * g.k;
-    const bool need_c = gap || pref || local_on;
+    const bool need_c = pref || local_on;
 
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const long long pbase = (long long)t * A_TILE;                    // source slot of the tile
-        const long long dbase = gap ? (long long)B.seg_off[t] : pbase;     // dense index of its first term
-        const int tcnt = gap ? B.seg_off[t + 1] - B.seg_off[t] : (int)min((long long)A_TILE, n - pbase);
+        const long long pbase = B.sphys[t];
+        const int tcnt = B.soff[t + 1] - B.soff[t];
         bool emit[A_ITEMS];
         Key<NW> key[A_ITEMS];
 #pragma unroll
@@ -122,13 +124,9 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
             const int idx = it * A_THREADS + tid;
             emit[it] = false;
             if (idx < tcnt) {
-                key[it] = load_key<NW>(Zs, Xs, pbase + idx);
+                key[it] = load_key<NW>(Z, X, pbase + idx);
                 double c = 0.0;
-                if (need_c) c = Cs[pbase + idx];
-                if (gap) {
-                    store_key<NW>(Zd, Xd, dbase + idx, key[it]);
-                    Cd[dbase + idx] = c;
-                }
+                if (need_c) c = C[pbase + idx];
                 Key<NW> q;
                 double sg;
                 if (rotate_term<NW>(key[it], g, &q, &sg)) {
@@ -181,7 +179,7 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
                 const int j = wtot[it * (A_THREADS / 32) + warp] + lpre[it];
 #pragma unroll
                 for (int w = 0; w < NW; ++w) { skz[w * A_TILE + j] = key[it].z[w]; skx[w * A_TILE + j] = key[it].x[w]; }
-                B.srcidx[pbase + j] = (int)(dbase + it * A_THREADS + tid);
+                B.srcidx[pbase + j] = (int)(pbase + it * A_THREADS + tid);
             }
         }
         __syncthreads();
@@ -262,7 +260,7 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     if (tid == 0) g = B.gens[rot];
     __syncthreads();
     const long long n = S->n;
-    const int ntiles = S->gapped ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
+    const int ntiles = (int)S->nseg;
     const int tpt = (ntiles + S_THREADS - 1) / S_THREADS;
     const int t0 = min(tid * tpt, ntiles), t1 = min(t0 + tpt, ntiles);
     // tile offsets
@@ -350,6 +348,8 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
 }
 
 // ---------------------------------------------------------------- A3 permute
+
+// ---------------------------------------------------------------- A3 permute
 // Thresholds are processed in groups of TAUV: per group one vector forward
 // max-scan and one vector backward min-scan of per-thread aggregates, then each
 // thread re-scans its A_ITEMS items in registers.
@@ -367,15 +367,14 @@ __global__ void __launch_bounds__(A_THREADS, 2) k_permute(Bufs B) {
     const int tid = threadIdx.x;
     if (tid == 0) g = B.gens[rot];
     __syncthreads();
-    const long long n = S->n;
     const long long atot = S->a;
-    const int ntiles = S->gapped ? (int)S->nseg : (int)((n + A_TILE - 1) / A_TILE);
+    const int ntiles = (int)S->nseg;
     const int ntau = 2 * g.k;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int cnt = B.aggA[t].count;
         if (cnt == 0) continue;
         const int off = B.offA[t];
-        const long long base = (long long)t * A_TILE;
+        const long long base = B.sphys[t];
         for (int j = tid; j < cnt; j += A_THREADS) { smeta[j] = B.meta[base + j]; ssrc[j] = B.srcidx[base + j]; }
         __syncthreads();
         const int j0 = tid * A_ITEMS;
@@ -460,7 +459,7 @@ template <int NW, int MODE>
 __device__ __forceinline__ Key<NW> v_key(const Bufs &B, const GenRec &g, const u64 *Z, const u64 *X, long long k) {
     if constexpr (MODE == 0) {
         int p = B.src[k];
-        if (p < 0 || p >= B.S->n) { atomicOr(&B.S->err, ERR_BOUNDS); p = 0; }
+        if (p < 0 || p >= B.cap) { atomicOr(&B.S->err, ERR_BOUNDS); p = 0; }
         Key<NW> P = load_key<NW>(Z, X, p);
 #pragma unroll
         for (int w = 0; w < NW; ++w) { P.z[w] ^= g.gz[w]; P.x[w] ^= g.gx[w]; }
@@ -477,9 +476,11 @@ __device__ __forceinline__ long long v_count(const DevState *S) {
 
 // ---------------------------------------------------------------- P partition
 // Merge-path split of (live, appended) at every multiple of B_D, one warp per
-// split: a 33-ary search (each round the 32 lanes probe 32 interior points of
-// the current range), so a split costs ~log_33(n) rounds of two dependent loads
-// (src[k], then the live key) instead of log_2(n).
+// split: 33-ary searches (each round the 32 lanes probe 32 interior points), so a
+// split costs a few rounds of dependent loads instead of log_2(n).  For the
+// window-1 rotation the live set is a segment table: the search first finds the
+// segment by probing segment starts, then the position inside it, and records
+// the segment (split_k) for the merge.
 constexpr int P_THREADS = 256;
 
 template <int NW, int MODE>
@@ -497,20 +498,63 @@ __global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
     const int cur = S->cur;
     const u64 *Z = B.z[cur], *X = B.x[cur];
     const long long nsplit = max(1ll, (tot + B_D - 1) / B_D);
+    const int nseg = MODE == 0 ? (int)S->nseg : 0;
     const int lane = threadIdx.x & 31;
     const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    // pred(i): live[i] precedes appended[d-i-1] in merged order (live first on ties)
-    auto pred = [&](long long d, long long i) {
-        return !key_lt<NW>(v_key<NW, MODE>(B, g, Z, X, d - i - 1), load_key<NW>(Z, X, i));
+    // pred(i): live element i (at physical position p) precedes appended[d-i-1]
+    auto pred = [&](long long d, long long i, long long p) {
+        return !key_lt<NW>(v_key<NW, MODE>(B, g, Z, X, d - i - 1), load_key<NW>(Z, X, p));
     };
     for (long long s = warp0; s <= nsplit; s += nwarps) {
         const long long d = min(s * (long long)B_D, tot);
         long long lo = max(0ll, d - a), hi = min(d, n);
+        long long seg_lo = 0, pbase = 0;          // dense start / physical base of the segment searched
+        int kseg = 0;
+        if constexpr (MODE == 0) {
+            // level 1: first segment k whose start is not below the split (Q(k) false)
+            auto Q = [&](int k) {
+                const long long sk = B.soff[k];
+                if (sk < lo) return true;
+                if (sk >= hi) return false;
+                return pred(d, sk, B.sphys[k]);
+            };
+            int klo = 0, khi = nseg;
+            while (khi - klo > 32) {
+                const long long span = khi - klo;
+                const int p = klo + (int)((span * (lane + 1)) / 33);
+                const unsigned m = __ballot_sync(0xffffffffu, !Q(p));
+                if (m == 0) {
+                    klo = __shfl_sync(0xffffffffu, p, 31) + 1;
+                } else {
+                    const int fl = __ffs(m) - 1;
+                    const int pf = __shfl_sync(0xffffffffu, p, fl);
+                    const int pprev = __shfl_sync(0xffffffffu, p, fl > 0 ? fl - 1 : 0);
+                    khi = pf;
+                    if (fl > 0) klo = pprev + 1;
+                }
+            }
+            {
+                const int p = klo + lane;
+                const unsigned m = __ballot_sync(0xffffffffu, p < khi && !Q(p));
+                klo = m ? klo + (__ffs(m) - 1) : khi;
+            }
+            const int K = klo - 1;                 // last segment whose start precedes the split
+            if (K < 0) {
+                hi = lo;                           // the split is at dense index 0
+            } else {
+                seg_lo = B.soff[K];
+                pbase = B.sphys[K];
+                lo = max(lo, seg_lo + 1);
+                hi = min(hi, (long long)B.soff[K + 1]);
+            }
+            kseg = K < 0 ? 0 : K;
+        }
+        // level 2 (or the whole search for dense live): first i in [lo, hi) with pred false
         while (hi - lo > 32) {
             const long long span = hi - lo;
             const long long p = lo + (span * (lane + 1)) / 33;
-            const bool f = !pred(d, p);
+            const bool f = !pred(d, p, pbase + p - seg_lo);
             const unsigned m = __ballot_sync(0xffffffffu, f);
             if (m == 0) {
                 lo = __shfl_sync(0xffffffffu, p, 31) + 1;
@@ -524,28 +568,35 @@ __global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
         }
         {
             const long long p = lo + lane;
-            const bool f = p < hi && !pred(d, p);
+            const bool f = p < hi && !pred(d, p, pbase + p - seg_lo);
             const unsigned m = __ballot_sync(0xffffffffu, f);
             lo = m ? lo + (__ffs(m) - 1) : hi;
         }
         if (lane == 0) {
             long long i = lo, j = d - lo;
+            if constexpr (MODE == 0) {
+                // segment holding dense index i (nseg when i == n)
+                if (i >= n) kseg = nseg;
+                else if (nseg > 0 && i >= B.soff[kseg + 1]) kseg = kseg + 1;
+            }
             // keep an equal-key run (live element followed by its appends) in one tile
             if (j < a && (i > 0 || j > 0)) {
                 Key<NW> last;
+                const long long pim1 = pbase + (i - 1) - seg_lo;   // live i-1 lies in the segment searched
                 if (j > 0 && i > 0) {
-                    const Key<NW> lv = load_key<NW>(Z, X, i - 1);
+                    const Key<NW> lv = load_key<NW>(Z, X, pim1);
                     const Key<NW> vv = v_key<NW, MODE>(B, g, Z, X, j - 1);
                     last = key_lt<NW>(vv, lv) ? lv : vv;
                 } else if (j > 0) {
                     last = v_key<NW, MODE>(B, g, Z, X, j - 1);
                 } else {
-                    last = load_key<NW>(Z, X, i - 1);
+                    last = load_key<NW>(Z, X, pim1);
                 }
                 while (j < a && key_eq<NW>(v_key<NW, MODE>(B, g, Z, X, j), last)) ++j;
             }
             B.split_i[s] = (int)i;
             B.split_j[s] = (int)j;
+            if constexpr (MODE == 0) B.split_k[s] = kseg;
         }
     }
 }
@@ -553,6 +604,7 @@ __global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
 // ---------------------------------------------------------------- B merge
 constexpr int B_VPT = B_CAP / B_THREADS;   // staged inputs per thread (10)
 constexpr int B_HALF = B_VPT;              // loads issued in one batch per tile
+constexpr int B_SEGL = 256;                // live segments of a tile held in shared memory
 
 template <int NW>
 constexpr size_t merge_smem_bytes() {
@@ -626,6 +678,7 @@ __device__ __forceinline__ double chan_lite(int kind, const u64 *mask, const dou
 // (live, appended).  Each CTA loops over tiles taken in order from a counter;
 // while warp 0 resolves the tile's output offset by decoupled look-back, the
 // other warps already issue the next tile's global loads into registers.
+
 template <int NW, int MODE>
 __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     DevState *S = B.S;
@@ -637,6 +690,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     __shared__ double s_red[3][B_THREADS / 32];
     __shared__ unsigned s_base;
     __shared__ double s_expw[130], s_expxw[130], s_ch[3][130];
+    __shared__ int s_so[B_SEGL], s_sp[B_SEGL];   // live segment list of the tile (MODE 0)
     extern __shared__ u64 sm[];
     u64 *skz = sm;                                                    // [NW][B_CAP]
     u64 *skx = skz + NW * B_CAP;                                      // [NW][B_CAP]
@@ -672,6 +726,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     u64 *OZ = B.z[cur ^ 1], *OX = B.x[cur ^ 1];
     double *OC = B.c[cur ^ 1];
     const int nsplit = (int)max(1ll, (tot + B_D - 1) / B_D);
+    const int nseg = MODE == 0 ? (int)S->nseg : 0;
     const unsigned epoch = S->epoch;
     const bool pref = MODE == 0 && n > S->acap_logical;
     const u64 ket[2] = {P.ket[0], P.ket[1]};
@@ -690,8 +745,29 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
         const int i0 = B.split_i[t], j0 = B.split_j[t];
         const int i1 = B.split_i[t + 1], j1 = B.split_j[t + 1];
         int nl = i1 - i0, nv = j1 - j0;
-        const bool tbad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
+        bool tbad = (nl + nv > B_CAP) || nl < 0 || nv < 0 || i0 < 0 || j0 < 0 || i1 > n || j1 > a;
         if (tbad) { nl = 0; nv = 0; }
+        int ks = 0, nsg = 1;
+        const int *so = s_so, *sp = s_sp;
+        if constexpr (MODE == 0) {
+            // segments ks..ke hold the tile's live range [i0, i1): ks holds i0, ke
+            // holds i1 (ke = nseg when i1 = n); every segment before ke holds one
+            // of its terms, so nsg <= nl + 1
+            ks = B.split_k[t];
+            const int ke = B.split_k[t + 1];
+            if (ks < 0 || ke > nseg || ke < ks) { tbad = true; nl = 0; nv = 0; ks = 0; }
+            else nsg = ke - ks + 1;
+            if (nsg <= B_SEGL) {
+                for (int k = tid; k < nsg; k += B_THREADS) {
+                    s_so[k] = B.soff[ks + k];
+                    s_sp[k] = ks + k < nseg ? B.sphys[ks + k] : 0;
+                }
+            } else {
+                so = B.soff + ks;
+                sp = B.sphys + ks;
+            }
+            __syncthreads();
+        }
         const int ntot = nl + nv;
         PHASE_START();
         // ---- stage the tile, two batches of loads each issued before its shared
@@ -710,7 +786,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
                 if constexpr (MODE == 0) {
                     if (e >= nl && e < ntot) {
                         int p = B.src[j0 + e - nl];
-                        if (p < 0 || p >= n) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
+                        if (p < 0 || p >= B.cap) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
                         srcp[q] = p;
                     }
                 }
@@ -719,8 +795,19 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
             for (int q = 0; q < B_HALF; ++q) {
                 const int e = tid + (hb * B_HALF + q) * B_THREADS;
                 if (e < nl) {
-                    kk[q] = load_key<NW>(Z, X, i0 + e);
-                    cc[q] = C[i0 + e];
+                    long long p = i0 + e;
+                    if constexpr (MODE == 0) {
+                        // physical position: the last segment starting at or before i0 + e
+                        int lo = 0, hi = nsg - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (so[mid] <= i0 + e) lo = mid; else hi = mid - 1;
+                        }
+                        p = (long long)sp[lo] + (i0 + e - so[lo]);
+                        if (p < 0 || p >= B.cap) { atomicOr(&S->err, ERR_BOUNDS); p = 0; }
+                    }
+                    kk[q] = load_key<NW>(Z, X, p);
+                    cc[q] = C[p];
                 } else if (e < ntot) {
                     if constexpr (MODE == 0) {
                         kk[q] = load_key<NW>(Z, X, srcp[q]);
@@ -827,8 +914,8 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
         const int loff = block_excl_scan<B_THREADS>(kept, 0, OpSum(), s_sc, &tkept);  // ends with a barrier
         PHASE_MARK(3);
         if constexpr (MODE == 0) {
-            // window-1 merge: the tile's survivors go to its own SEG-term slot (the
-            // gapped layout that the next classify compacts), no look-back wait
+            // window-1 merge: the tile's survivors go to its own SEG-term slot of
+            // the other set (k_commit lists the non-empty slots), no look-back wait
             if (tid == 0) { s_base = (unsigned)((long long)t * SEG); B.kcnt[t] = tkept; }
         } else if (warp == 0) {
             const unsigned ex = lookback_warp(B.tstat, t, epoch, (unsigned)tkept, &S->err);
@@ -921,18 +1008,23 @@ __global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
         }
     }
     __shared__ long long s_tot;
+    __shared__ int s_nseg;
     __shared__ int s_scan[256 / 32 + 1];
     if constexpr (MODE == 0) {
-        // window-1 merge: segment table of the gapped output (dense start of each
-        // tile's survivors), scanned in tile order
+        // window-1 merge: the segment table of the output, i.e. its non-empty tile
+        // slots in tile order with the dense index of their first term
         const int per = (nsplit + 255) / 256;
         const int t0 = min(tid * per, nsplit), t1 = min(t0 + per, nsplit);
-        int loc = 0;
-        for (int tt = t0; tt < t1; ++tt) loc += B.kcnt[tt];
-        int all;
+        int loc = 0, lne = 0;
+        for (int tt = t0; tt < t1; ++tt) { const int k = B.kcnt[tt]; loc += k; lne += k > 0; }
+        int all, nne;
         int run = block_excl_scan<256>(loc, 0, OpSum(), s_scan, &all);
-        for (int tt = t0; tt < t1; ++tt) { B.seg_off[tt] = run; run += B.kcnt[tt]; }
-        if (tid == 0) { B.seg_off[nsplit] = all; s_tot = all; }
+        int pos = block_excl_scan<256>(lne, 0, OpSum(), s_scan, &nne);
+        for (int tt = t0; tt < t1; ++tt) {
+            const int k = B.kcnt[tt];
+            if (k > 0) { B.sphys[pos] = tt * SEG; B.soff[pos] = run; ++pos; run += k; }
+        }
+        if (tid == 0) { B.soff[nne] = all; s_tot = all; s_nseg = nne; }
         __syncthreads();
     } else {
         if (tid == 0) s_tot = (long long)(unsigned)(st_load(B.tstat + (nsplit - 1)) & 0xffffffffu);
@@ -942,11 +1034,12 @@ __global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
         const bool pref = MODE == 0 && n > S->acap_logical;
         const long long total = s_tot;
         S->n = total;
+        S->cur ^= 1;
         if (MODE == 0) {
-            S->gapped = 1;
-            S->nseg = nsplit;
+            S->seg_dense = 0;
+            S->nseg = s_nseg;
         } else {
-            S->cur ^= 1;
+            S->seg_dense = 1;   // dense output; the segment table is rebuilt before the next window-1 run
         }
         S->merge_in += tot;
         S->merge_out += total;
@@ -977,22 +1070,35 @@ __global__ void __launch_bounds__(256) k_commit(Bufs B, int argflags) {
     }
 }
 
-// Compacts a gapped window-1 merge output (set cur^1, segment table seg_off)
-// into the dense set cur; k_densify_commit then marks the state dense.
+// Segment table of a dense live set (set cur): segment k = terms [k SEG, (k+1) SEG).
+__global__ void k_segdense(Bufs B) {
+    DevState *S = B.S;
+    if (!S->seg_dense) return;    // a segmented live set keeps the table its merge wrote
+    const long long n = S->n;
+    const int nseg = (int)((n + SEG - 1) / SEG);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= nseg; k += gridDim.x * blockDim.x) {
+        if (k < nseg) B.sphys[k] = k * SEG;
+        B.soff[k] = k < nseg ? k * SEG : (int)n;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { S->nseg = nseg; S->seg_dense = 1; }
+}
+
+// Copies a segmented live set (set cur) densely into set cur^1; k_densify_commit
+// then makes that the live set.
 template <int NW>
 __global__ void k_densify(Bufs B) {
     DevState *S = B.S;
-    if (!S->gapped) return;
+    if (S->seg_dense) return;
     const int cur = S->cur;
     const int nseg = (int)S->nseg;
-    const u64 *Zs = B.z[cur ^ 1], *Xs = B.x[cur ^ 1];
-    const double *Cs = B.c[cur ^ 1];
-    u64 *Zd = B.z[cur], *Xd = B.x[cur];
-    double *Cd = B.c[cur];
-    for (int t = blockIdx.x; t < nseg; t += gridDim.x) {
-        const long long d0 = B.seg_off[t];
-        const int cnt = B.seg_off[t + 1] - B.seg_off[t];
-        const long long p0 = (long long)t * SEG;
+    const u64 *Zs = B.z[cur], *Xs = B.x[cur];
+    const double *Cs = B.c[cur];
+    u64 *Zd = B.z[cur ^ 1], *Xd = B.x[cur ^ 1];
+    double *Cd = B.c[cur ^ 1];
+    for (int k = blockIdx.x; k < nseg; k += gridDim.x) {
+        const long long d0 = B.soff[k];
+        const int cnt = B.soff[k + 1] - B.soff[k];
+        const long long p0 = B.sphys[k];
         for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
             store_key<NW>(Zd, Xd, d0 + e, load_key<NW>(Zs, Xs, p0 + e));
             Cd[d0 + e] = Cs[p0 + e];
@@ -1001,7 +1107,8 @@ __global__ void k_densify(Bufs B) {
 }
 
 __global__ void k_densify_commit(Bufs B) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) B.S->gapped = 0;
+    DevState *S = B.S;
+    if (threadIdx.x == 0 && blockIdx.x == 0 && !S->seg_dense) { S->cur ^= 1; S->seg_dense = 1; }
 }
 
 }  // namespace pp
