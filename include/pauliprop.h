@@ -120,6 +120,36 @@ int pp_evolve1(pp_spv *h, const void *gz, const void *gx, double cos_theta, doub
  * host-computed cos(θ_i), sin(θ_i) (spv_evolve.jl:341-342). */
 int pp_evolve(pp_spv *h, const void *gz, const void *gx, const double *cosv, const double *sinv,
               int64_t L, const pp_evolve_opts *opts);
+/* Batched instances for pp_evolve_batch.  Instance i's terms are 128-bit words
+ * (the handle is created with N > 64): bits 0..63 of z / x are the instance's own
+ * nq-qubit word (as a UInt64 SparsePauliVector of N = nq would hold it), bits
+ * 64..127 of z hold i, bits 64..127 of x are zero. */
+typedef struct {
+    int64_t ninst;                /* instances */
+    int32_t nq;                   /* qubits of every instance (1..64) */
+    int32_t ncol;                 /* angle columns */
+    const int32_t *acol;          /* [L] angle column of each rotation */
+    const double *cosv, *sinv;    /* [ninst * ncol] cos / sin of instance i's column j at [i * ncol + j] */
+    const int64_t *rot_end;       /* [ninst] rotations instance i runs: the first rot_end[i] of the L */
+    int32_t keep_finished;        /* 0: an instance's terms leave the vector when it finishes */
+    int32_t pad;
+    double *expect_out;           /* [ninst] <ket|O_i|ket> after its last rotation (nullable) */
+    double *t_done;               /* [ninst] device seconds from the call's start to that result (nullable) */
+    int64_t *n_final;             /* [ninst] terms of instance i after its last rotation (nullable) */
+} pp_batch;
+
+/* The sequence evolve! (spv_evolve.jl:312-387) of many independent vectors in one
+ * pass: equivalent, instance by instance, to evolve!(v_i, gens[1:rot_end[i]],
+ * angles_i; truncation) at window = 1 with an append capacity large enough that no
+ * early merge happens (spv_evolve.jl:356-362), plus opts->chan_kind applied after
+ * every chan_every-th rotation the instance runs (the channel acts on the nq
+ * instance qubits, or on opts->chan_mask's word 0).  gz/gx: L generators as
+ * 128-bit words acting on bits 0..nq-1 only.  The strict filter's weights count
+ * word 0 only.  opts may be NULL; window must be 1; local truncation, adaptive
+ * truncation and corrections are rejected.  No counterpart in the reference (its
+ * vectors evolve one at a time). */
+int pp_evolve_batch(pp_spv *h, const void *gz, const void *gx, int64_t L, const pp_batch *b,
+                    const pp_evolve_opts *opts);
 /* coeff_clip! / weight_clip! / x_weight_clip! / majorana_weight_clip! /
  * weight_damped_clip! / x_weight_damped_clip! and the compilable truncate!
  * (spv_evolve.jl:13-26, 59-65) -> _compact_spv! (spv_kernels.jl:395-408). */

@@ -20,6 +20,7 @@
 
 #include "../../include/pauliprop.h"
 #include "kernels_general.cuh"
+#include "kernels_batch.cuh"
 
 using namespace pp;
 
@@ -86,6 +87,16 @@ struct pp_spv {
     long long *rec = nullptr;             // per-rotation counters (window-1 WindowCounters)
     long long rec_cap = 0;
     bool rec_on = false;
+    // batched instances (pp_evolve_batch)
+    double *bcos = nullptr, *bsin = nullptr;
+    long long *bend = nullptr;
+    long long btab_cap = 0, binst_cap = 0;
+    long long ninst = 0;
+    int ncol = 0;
+    bool batch_on = false;
+    int *hfin = nullptr;
+    double *hpart = nullptr, *heout = nullptr;
+    long long *hrange = nullptr, *hnout = nullptr;
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
     long long gexec_gen[3] = {-1, -1, -1};
 };
@@ -121,6 +132,8 @@ static Bufs make_bufs(pp_spv *h) {
     B.rec = h->rec_on ? h->rec : nullptr;
     B.sphys = h->sphys; B.soff = h->soff;
     B.kcnt = h->kcnt;
+    B.bcos = h->bcos; B.bsin = h->bsin; B.bend = h->bend;
+    B.ninst = h->ninst; B.ncol = h->ncol; B.batch = h->batch_on ? 1 : 0;
     B.S = h->S; B.P = h->P; B.gens = h->gens;
     return B;
 }
@@ -328,6 +341,7 @@ static void compile_filter(const pp_filter *f, DevFilter *d) {
     d->use_dw = F.dthresh_w >= 0.0;
     d->use_dxw = F.dthresh_xw >= 0.0;
     d->coeff_based = (F.thresh >= 0.0) || d->use_dw || d->use_dxw;
+    d->wlow = 0;
     for (int w = 0; w < 130; ++w) {
         d->expw[w] = std::exp(-F.alpha_w * (double)w);     // absc * exp(-alpha*w), spv_kernels.jl:73
         d->expxw[w] = std::exp(-F.alpha_xw * (double)w);   // spv_kernels.jl:76
@@ -548,7 +562,8 @@ extern "C" int pp_destroy(pp_spv *h) {
     void *ptrs[] = {h->z[0], h->z[1], h->x[0], h->x[1], h->c[0], h->c[1], h->srcidx, h->src, h->meta, h->aggA,
                     h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
-                    h->S, h->P, h->gens, h->rec, h->sphys, h->soff, h->kcnt, h->split_k};
+                    h->S, h->P, h->gens, h->rec, h->sphys, h->soff, h->kcnt, h->split_k,
+                    h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
@@ -672,11 +687,12 @@ struct RunProf {
     long long launches = 0;
 };
 
-// Structured window-1 sequence: chunks of CHUNK_ROT rotations between state
-// read-backs; on ERR_OVERFLOW grow and resume at the rotation that stopped.
+// Structured window-1 sequence over rotations [start, L) (the device cursor
+// S->rot is at start): chunks of CHUNK_ROT rotations between state read-backs; on
+// ERR_OVERFLOW grow and resume at the rotation that stopped.
 template <int NW>
-static int run_struct(pp_spv *h, long long L, pp_counters *ctr, RunProf *prof) {
-    long long done = 0;
+static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof) {
+    long long done = start;
     const bool timed = prof->on || (ctr && (ctr->t_rotate || ctr->t_merge));
     std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
     bool table = false;            // the device segment table describes the (dense) live set
@@ -942,8 +958,8 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
             h->rec_cap = L;
         }
         if (want_rec != h->rec_on) { h->rec_on = want_rec; h->buf_gen++; }
-        if (h->NW == 1) TRY(run_struct<1>(h, L, ctr, &prof));
-        else TRY(run_struct<2>(h, L, ctr, &prof));
+        if (h->NW == 1) TRY(run_struct<1>(h, 0, L, ctr, &prof));
+        else TRY(run_struct<2>(h, 0, L, ctr, &prof));
         if (want_rec) {
             std::vector<long long> rec((size_t)(4 * L));
             CU(cudaMemcpy(rec.data(), h->rec, 4 * L * sizeof(long long), cudaMemcpyDeviceToHost));
@@ -1085,4 +1101,216 @@ extern "C" int pp_device_bytes(pp_spv *h, int64_t *bytes) {
     if (!h || !bytes) return fail(PP_ARGUMENT_ERROR, "null argument");
     *bytes = h->bytes;
     return PP_OK;
+}
+
+// ------------------------------------------------------------------ batched instances
+template <typename T>
+static int ensure_buf(pp_spv *h, T **p, long long need, long long *cap) {
+    if (need <= *cap && *p) return PP_OK;
+    TRY(dalloc(h, p, need));
+    *cap = need;
+    return PP_OK;
+}
+
+static int batch_impl(pp_spv *h, const void *gz, const void *gx, long long L, const pp_batch *b,
+                      const pp_evolve_opts &O, long long *acap_saved) {
+    const long long ninst = b->ninst;
+    const int ncol = b->ncol, nq = b->nq;
+    std::vector<long long> ends((size_t)ninst);
+    for (long long i = 0; i < ninst; ++i) {
+        ends[i] = b->rot_end[i];
+        if (ends[i] < 0 || ends[i] > L) return fail(PP_ARGUMENT_ERROR, "rot_end must lie in 0..L");
+    }
+    // parameters: strict filter over the instance word, no local filter, channel on the instance qubits
+    DevParams *P = h->Ph;
+    compile_filter(O.strict, &P->strict);
+    P->strict.wlow = 1;
+    compile_filter(nullptr, &P->local);
+    P->local_active = 0;
+    compile_filter(nullptr, &P->clip);   // the harvest compaction keeps every term of running instances
+    P->corr_kind = 0;
+    load_word(O.ket, 2, P->ket);
+    P->ket[1] = 0;
+    P->chan_kind = -1;
+    if (O.chan_kind >= 0) {
+        u64 m[2] = {nq == 64 ? ~0ull : ((1ull << nq) - 1ull), 0ull};
+        if (O.chan_mask) {
+            load_word(O.chan_mask, 2, m);
+            m[1] = 0;
+        }
+        TRY(build_channel(h, O.chan_kind, O.chan_prm, m, P));
+    }
+    TRY(upload_params(h));
+    // instance tables and harvest workspaces
+    long long tcap = h->btab_cap, icap = h->binst_cap;
+    TRY(ensure_buf(h, &h->bcos, ninst * ncol, &tcap));
+    tcap = h->btab_cap;
+    TRY(ensure_buf(h, &h->bsin, ninst * ncol, &tcap));
+    h->btab_cap = tcap;
+    if (ninst > h->binst_cap || !h->bend) {
+        TRY(dalloc(h, &h->bend, ninst));
+        TRY(dalloc(h, &h->hfin, ninst));
+        TRY(dalloc(h, &h->hpart, ninst * HV_CHUNKS));
+        TRY(dalloc(h, &h->heout, ninst));
+        TRY(dalloc(h, &h->hrange, 2 * ninst));
+        TRY(dalloc(h, &h->hnout, ninst));
+        icap = ninst;
+    }
+    h->binst_cap = icap;
+    CU(cudaMemcpyAsync(h->bcos, b->cosv, ninst * ncol * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->bsin, b->sinv, ninst * ncol * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->bend, ends.data(), ninst * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+    h->batch_on = true;
+    h->ninst = ninst;
+    h->ncol = ncol;
+    h->rec_on = false;
+    h->buf_gen++;
+    // generators: the instance qubits only; the angle column of each rotation
+    if (L > 0) {
+        TRY(ensure_gens(h, L));
+        std::vector<GenRec> G((size_t)L);
+        for (long long i = 0; i < L; ++i) {
+            u64 wz[2] = {0, 0}, wx[2] = {0, 0};
+            memcpy(wz, (const char *)gz + i * 16, 16);
+            memcpy(wx, (const char *)gx + i * 16, 16);
+            if (wz[1] || wx[1] || (nq < 64 && ((wz[0] | wx[0]) >> nq)))
+                return fail(PP_ARGUMENT_ERROR, "generators must act on the instance qubits only");
+            if (b->acol[i] < 0 || b->acol[i] >= ncol) return fail(PP_ARGUMENT_ERROR, "acol out of range");
+            bool st = true;
+            TRY(make_gen(h, wz, wx, 1.0, 0.0, &G[i], &st));
+            if (!st) return fail(PP_NOT_IMPLEMENTED, "batched instances need generators of at most 16 mask levels");
+            G[i].acol = b->acol[i];
+        }
+        if (O.chan_kind >= 0) {
+            if (O.chan_every > 0) {
+                for (long long i = O.chan_every - 1; i < L; i += O.chan_every) G[i].flags |= GEN_CHANNEL;
+            } else {
+                G[L - 1].flags |= GEN_CHANNEL;
+            }
+        }
+        memcpy(h->gens_h, G.data(), L * sizeof(GenRec));
+        CU(cudaMemcpyAsync(h->gens, h->gens_h, L * sizeof(GenRec), cudaMemcpyHostToDevice, h->stream));
+    }
+    // state: no early merges (every instance has an unbounded append capacity)
+    DevState st;
+    TRY(read_state(h, &st));
+    *acap_saved = st.acap_logical;
+    st.acap_logical = 1ll << 62;
+    st.rot = 0;
+    st.rot_end = 0;
+    st.created = st.merge_in = st.merge_out = st.early = 0;
+    st.npref = 0;
+    st.live_in = 0;
+    st.peak = 0;
+    st.measure_valid = 0;
+    st.b_tile_ctr = 0;
+    st.g_tile_ctr = 0;
+    TRY(write_state(h, &st));
+    TRY(ensure_live(h, 3 * st.n + 2 * SEG));
+    // harvest points: the distinct instance ends, in order
+    std::vector<long long> pts(ends);
+    std::sort(pts.begin(), pts.end());
+    pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
+    std::vector<cudaEvent_t> ev(pts.size() + 1);
+    for (auto &e : ev) cudaEventCreate(&e);
+    struct EvGuard {
+        std::vector<cudaEvent_t> &v;
+        ~EvGuard() { for (auto e : v) cudaEventDestroy(e); }
+    } evg{ev};
+    RunProf prof;
+    prof.on = O.profile != 0;
+    CU(cudaEventRecord(ev[0], h->stream));
+    long long done = 0;
+    std::vector<int> fin;
+    fin.reserve((size_t)ninst);
+    for (size_t k = 0; k < pts.size(); ++k) {
+        const long long r = pts[k];
+        if (r > done) {
+            TRY(read_state(h, &st));
+            st.rot_end = r;
+            TRY(write_state(h, &st));
+            TRY(run_struct<2>(h, done, r, nullptr, &prof));
+            done = r;
+        }
+        fin.clear();
+        for (long long i = 0; i < ninst; ++i) if (ends[i] == r) fin.push_back((int)i);
+        const int nfin = (int)fin.size();
+        CU(cudaMemcpyAsync(h->hfin, fin.data(), nfin * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+        Bufs B = make_bufs(h);
+        k_harvest_part<<<dim3(HV_CHUNKS, nfin), HV_THREADS, 0, h->stream>>>(B, h->hfin, h->hpart, h->hrange);
+        k_harvest_fin<<<(nfin + 127) / 128, 128, 0, h->stream>>>(h->hfin, nfin, h->hpart, h->hrange, h->heout,
+                                                                 h->hnout);
+        prof.launches += 2;
+        if (!b->keep_finished) {
+            TRY(read_state(h, &st));
+            st.an = 0;
+            TRY(write_state(h, &st));
+            launch_merge<2, 2>(h, B, GEN_HARVEST);
+            prof.launches += 3;
+        }
+        CU(cudaEventRecord(ev[k + 1], h->stream));
+        TRY(sync_check(h));
+        TRY(read_state(h, &st));
+        TRY(check_err(h, st));
+    }
+    if (b->expect_out)
+        CU(cudaMemcpyAsync(b->expect_out, h->heout, ninst * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (b->n_final)
+        CU(cudaMemcpyAsync(b->n_final, h->hnout, ninst * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (b->t_done) {
+        for (long long i = 0; i < ninst; ++i) {
+            const size_t k = std::lower_bound(pts.begin(), pts.end(), ends[i]) - pts.begin();
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[0], ev[k + 1]);
+            b->t_done[i] = ms * 1e-3;
+        }
+    }
+    TRY(read_state(h, &st));
+    if (O.stats_out) {
+        double *so = O.stats_out;
+        for (int i = 0; i < PP_STATS_LEN; ++i) so[i] = 0.0;
+        so[PP_STAT_TERMS_IN] = (double)st.live_in;
+        so[PP_STAT_CREATED] = (double)st.created;
+        so[PP_STAT_MERGE_IN] = (double)st.merge_in;
+        so[PP_STAT_MERGE_OUT] = (double)st.merge_out;
+        so[PP_STAT_PEAK] = (double)st.peak;
+        so[PP_STAT_T_ROTATE] = prof.t_rotate;
+        so[PP_STAT_T_MERGE] = prof.t_merge;
+        so[PP_STAT_LAUNCHES] = (double)prof.launches;
+        so[PP_STAT_T_PARTITION] = prof.t_partition;
+    }
+    return PP_OK;
+}
+
+extern "C" int pp_evolve_batch(pp_spv *h, const void *gz, const void *gx, int64_t L, const pp_batch *b,
+                               const pp_evolve_opts *opts) {
+    if (!h || !b) return fail(PP_ARGUMENT_ERROR, "null argument");
+    if (h->NW != 2) return fail(PP_ARGUMENT_ERROR, "batched instances need a handle with 128-bit words (N > 64)");
+    if (L < 0 || b->ninst < 1 || b->ninst > (1ll << 30) || b->ncol < 1 || b->nq < 1 || b->nq > 64)
+        return fail(PP_ARGUMENT_ERROR, "need L >= 0, 1 <= ninst <= 2^30, ncol >= 1, 1 <= nq <= 64");
+    if ((L > 0 && (!gz || !gx || !b->acol)) || !b->cosv || !b->sinv || !b->rot_end)
+        return fail(PP_ARGUMENT_ERROR, "null array");
+    pp_evolve_opts O;
+    memset(&O, 0, sizeof O);
+    O.window = 1;
+    O.chan_kind = -1;
+    if (opts) O = *opts;
+    if (O.window != 1) return fail(PP_ARGUMENT_ERROR, "batched instances run at window = 1");
+    if (!filter_is_nofilter(O.local)) return fail(PP_ARGUMENT_ERROR, "batched instances take no local_truncation");
+    if (O.strict_kind != 0 || O.corr_kind != 0)
+        return fail(PP_NOT_IMPLEMENTED, "batched instances support compiled truncations and NoCorrection only");
+    long long acap = -1;
+    int r = batch_impl(h, gz, gx, L, b, O, &acap);
+    // back to a plain vector whatever happened
+    h->batch_on = false;
+    h->buf_gen++;
+    if (acap >= 0) {
+        DevState st;
+        if (read_state(h, &st) == PP_OK) {
+            st.acap_logical = acap;
+            write_state(h, &st);
+        }
+    }
+    return r;
 }

@@ -35,6 +35,7 @@ struct DevFilter {
     double thresh, dthresh_w, dthresh_xw;
     int use_mw, use_dw, use_dxw;
     int coeff_based;              // 1 if any criterion reads |c|
+    int wlow;                     // 1: weights count z/x word 0 only (batched instances keep a tag in z word 1)
     double expw[130];             // exp(-alpha_w * w),  w = popcount(z|x) in 0..128
     double expxw[130];            // exp(-alpha_xw * w), w = popcount(x)   in 0..128
 };
@@ -58,11 +59,12 @@ struct GenRec {
     int ng;                       // popcount(gz & gx)
     int k;                        // number of mask levels
     int flags;                    // GEN_MEASURE | GEN_CHANNEL
-    int pad;
+    int acol;                     // batched instances: column of this rotation's angle in the instance table
     short level[KMAX];            // mask levels, strictly descending
 };
 constexpr int GEN_MEASURE = 1;    // reduce <ket|O|ket> partials after this rotation
 constexpr int GEN_CHANNEL = 2;    // apply the channel in this rotation's merge epilogue
+constexpr int GEN_HARVEST = 4;    // compaction (MODE 2) also drops batched instances that have finished
 
 struct DevState {
     long long n;                  // live terms
@@ -218,18 +220,36 @@ __device__ __forceinline__ long long majorana(const Key<NW> &k) {
     }
 }
 
+// Majorana weight of the term; with wlow (batched instances) over word 0 alone,
+// which is the 64-bit word an instance of N <= 64 qubits has on its own.
+template <int NW>
+__device__ __forceinline__ long long majorana_f(const Key<NW> &k, int wlow) {
+    if constexpr (NW == 2) {
+        if (wlow) {
+            Key<1> k1;
+            k1.z[0] = k.z[0];
+            k1.x[0] = k.x[0];
+            return majorana<1>(k1);
+        }
+    }
+    return majorana<NW>(k);
+}
+
 // should_drop (spv_kernels.jl:64-79).
 template <int NW>
 __device__ __forceinline__ bool should_drop(const DevFilter &f, const Key<NW> &k, double absc) {
     if (absc <= f.thresh) return true;
-    u64 o[NW];
+    u64 o[NW], xx[NW];
 #pragma unroll
-    for (int w = 0; w < NW; ++w) o[w] = k.z[w] | k.x[w];
+    for (int w = 0; w < NW; ++w) { o[w] = k.z[w] | k.x[w]; xx[w] = k.x[w]; }
+    if constexpr (NW == 2) {
+        if (f.wlow) { o[1] = 0; xx[1] = 0; }
+    }
     int wt = popc_w<NW>(o);
     if (wt > f.wmax) return true;
-    int xw = popc_w<NW>(k.x);
+    int xw = popc_w<NW>(xx);
     if (xw > f.xwmax) return true;
-    if (f.use_mw && majorana<NW>(k) > f.mwmax) return true;
+    if (f.use_mw && majorana_f<NW>(k, f.wlow) > f.mwmax) return true;
     if (f.use_dw && __dmul_rn(absc, f.expw[wt]) <= f.dthresh_w) return true;
     if (f.use_dxw && __dmul_rn(absc, f.expxw[xw]) <= f.dthresh_xw) return true;
     return false;

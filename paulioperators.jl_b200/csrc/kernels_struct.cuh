@@ -68,6 +68,12 @@ struct Bufs {
     long long *rec;               // nullable: per-rotation counters [rot][4] (window 1)
     int *sphys, *soff;            // live segment table: physical base / dense start [nseg + 1]
     int *kcnt;                    // survivors per merge tile (window-1 merge)
+    // batched instances (NW = 2 only): the instance index of a term is its z word 1
+    const double *bcos, *bsin;    // [ninst * ncol] cos / sin of each instance's angle columns
+    const long long *bend;        // [ninst] rotations each instance runs
+    long long ninst;
+    int ncol;
+    int batch;                    // 1: the live set holds batched instances
     u64 *vz, *vx;
     double *vc;
     u64 *gstat;
@@ -80,6 +86,40 @@ constexpr int TAUV = 8;   // scan thresholds sharing one vector block scan
 
 __device__ __forceinline__ int tau_value(const GenRec &g, int tau) {
     return (int)g.level[tau >> 1] + (tau & 1);
+}
+
+// Rotation angle of a term at rotation `rot`: the generator's own cos/sin, or for
+// batched instances the term's instance's angle column; false when the instance
+// has finished (it no longer rotates, creates no sin branch and gets no channel).
+template <int NW>
+__device__ __forceinline__ bool term_angle(const Bufs &B, const GenRec &g, long long rot, const Key<NW> &k,
+                                           double *cv, double *sv) {
+    if constexpr (NW == 2) {
+        if (B.batch) {
+            const u64 t = k.z[1];
+            if (t >= (u64)B.ninst) { atomicOr(&B.S->err, ERR_BOUNDS); return false; }
+            if (rot >= B.bend[t]) return false;
+            const long long i = (long long)t * B.ncol + g.acol;
+            *cv = B.bcos[i];
+            *sv = B.bsin[i];
+            return true;
+        }
+    }
+    *cv = g.cosv;
+    *sv = g.sinv;
+    return true;
+}
+
+// A batched term whose instance ran its last rotation before `rot`.
+template <int NW>
+__device__ __forceinline__ bool term_finished(const Bufs &B, long long rot, const Key<NW> &k) {
+    if constexpr (NW == 2) {
+        if (B.batch) {
+            const u64 t = k.z[1];
+            return t >= (u64)B.ninst || rot >= B.bend[t];
+        }
+    }
+    return false;
 }
 
 // ---------------------------------------------------------------- A1 classify
@@ -128,12 +168,12 @@ __global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
                 double c = 0.0;
                 if (need_c) c = C[pbase + idx];
                 Key<NW> q;
-                double sg;
-                if (rotate_term<NW>(key[it], g, &q, &sg)) {
+                double sg, cv, sv;
+                if (rotate_term<NW>(key[it], g, &q, &sg) && term_angle<NW>(B, g, rot, key[it], &cv, &sv)) {
                     bool ok = true;
                     if (pref && should_drop<NW>(P.strict, key[it], fabs(c))) ok = false;
                     if (ok && local_on) {
-                        const double cn = __dmul_rn(sg * g.sinv, c);
+                        const double cn = __dmul_rn(sg * sv, c);
                         if (should_drop<NW>(P.local, q, fabs(cn))) ok = false;
                     }
                     emit[it] = ok;
@@ -622,14 +662,14 @@ __device__ __forceinline__ const DevFilter &merge_filter(const DevParams &P) {
 struct FLite {
     long long wmax, xwmax, mwmax;
     double thresh, dthresh_w, dthresh_xw;
-    int use_mw, use_dw, use_dxw;
+    int use_mw, use_dw, use_dxw, wlow;
 };
 
 __device__ __forceinline__ FLite flite(const DevFilter &f) {
     FLite r;
     r.wmax = f.wmax; r.xwmax = f.xwmax; r.mwmax = f.mwmax;
     r.thresh = f.thresh; r.dthresh_w = f.dthresh_w; r.dthresh_xw = f.dthresh_xw;
-    r.use_mw = f.use_mw; r.use_dw = f.use_dw; r.use_dxw = f.use_dxw;
+    r.use_mw = f.use_mw; r.use_dw = f.use_dw; r.use_dxw = f.use_dxw; r.wlow = f.wlow;
     return r;
 }
 
@@ -638,14 +678,17 @@ template <int NW>
 __device__ __forceinline__ bool drop_lite(const FLite &f, const double *sexpw, const double *sexpxw, const Key<NW> &k,
                                           double absc) {
     if (absc <= f.thresh) return true;
-    u64 o[NW];
+    u64 o[NW], xx[NW];
 #pragma unroll
-    for (int w = 0; w < NW; ++w) o[w] = k.z[w] | k.x[w];
+    for (int w = 0; w < NW; ++w) { o[w] = k.z[w] | k.x[w]; xx[w] = k.x[w]; }
+    if constexpr (NW == 2) {
+        if (f.wlow) { o[1] = 0; xx[1] = 0; }
+    }
     const int wt = popc_w<NW>(o);
     if (wt > f.wmax) return true;
-    const int xw = popc_w<NW>(k.x);
+    const int xw = popc_w<NW>(xx);
     if (xw > f.xwmax) return true;
-    if (f.use_mw && majorana<NW>(k) > f.mwmax) return true;
+    if (f.use_mw && majorana_f<NW>(k, f.wlow) > f.mwmax) return true;
     if (f.use_dw && __dmul_rn(absc, sexpw[wt]) <= f.dthresh_w) return true;
     if (f.use_dxw && __dmul_rn(absc, sexpxw[xw]) <= f.dthresh_xw) return true;
     return false;
@@ -730,6 +773,8 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     const unsigned epoch = S->epoch;
     const bool pref = MODE == 0 && n > S->acap_logical;
     const u64 ket[2] = {P.ket[0], P.ket[1]};
+    const long long rot = S->rot;
+    const bool harvest = MODE == 2 && (flags & GEN_HARVEST) != 0;
 
     auto skey = [&](int slot) {
         Key<NW> k;
@@ -827,15 +872,16 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
                 unsigned char dead = 0;
                 if constexpr (MODE == 0) {
                     Key<NW> qk;
-                    double sg = 0.0;
+                    double sg = 0.0, cv = 1.0, sv = 0.0;
                     const bool anti = rotate_term<NW>(k, g, &qk, &sg);
+                    const bool act = term_angle<NW>(B, g, rot, k, &cv, &sv);
                     if (e < nl) {
                         if (pref && drop_lite<NW>(fs, F.expw, F.expxw, k, fabs(c))) dead = 1;
-                        else if (anti) c = __dmul_rn(c, g.cosv);
+                        else if (anti && act) c = __dmul_rn(c, cv);
                         nalive += dead ? 0 : 1;
                     } else {
                         k = qk;
-                        c = __dmul_rn(sg * g.sinv, c);
+                        c = __dmul_rn(sg * sv, c);
                     }
                 }
 #pragma unroll
@@ -898,11 +944,16 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
                 have = true;
             }
             if (!have) continue;
-            if (drop_lite<NW>(fl, s_expw, s_expxw, kp, fabs(acc))) {
+            // a finished batched instance is left as its last merge wrote it: no
+            // filter, no channel (its terms passed its own last filter already)
+            const bool fin = term_finished<NW>(B, rot, kp);
+            if (!fin && drop_lite<NW>(fl, s_expw, s_expxw, kp, fabs(acc))) {
                 if (diag && do_meas) e_drop.add(sgn * acc);
                 continue;
             }
-            const double o = do_chan ? __dmul_rn(acc, chan_lite<NW>(chan_kind, chan_mask, s_ch[0], s_ch[1], s_ch[2], kp)) : acc;
+            if (harvest && fin) continue;
+            const bool ch = do_chan && !fin;
+            const double o = ch ? __dmul_rn(acc, chan_lite<NW>(chan_kind, chan_mask, s_ch[0], s_ch[1], s_ch[2], kp)) : acc;
             if (diag && do_meas) e_keep.add(sgn * o);
             outq[q] = o;
             slotq[q] = (unsigned short)sl;

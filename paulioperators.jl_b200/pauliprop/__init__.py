@@ -20,6 +20,7 @@ from .spv import (SparsePauliVector, WindowCounters, bit_flip_channel, bit_flip_
                   expectation_value, majorana_weight_clip_, pauli_channel, pauli_channel_,
                   phase_flip_channel_, power_table, truncate_, weight_clip_,
                   weight_damped_clip_, x_weight_clip_, x_weight_damped_clip_)
+from .batch import BatchResult, evolve_batch, split_instances, tagged_terms
 from . import circuits
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -67,6 +67,13 @@ class PPEvolveOpts(Structure):
                 ("profile", c_int32), ("pad2", c_int32)]
 
 
+class PPBatch(Structure):
+    _fields_ = [("ninst", c_int64), ("nq", c_int32), ("ncol", c_int32),
+                ("acol", c_void_p), ("cosv", c_void_p), ("sinv", c_void_p), ("rot_end", c_void_p),
+                ("keep_finished", c_int32), ("pad", c_int32),
+                ("expect_out", c_void_p), ("t_done", c_void_p), ("n_final", c_void_p)]
+
+
 PP_STATS_LEN = 16
 STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
         "t_rotate": 6, "t_merge": 7, "launches": 8, "t_partition": 9}
@@ -83,6 +90,8 @@ SIGNATURES = {
     "pp_evolve1": (c_int32, [c_void_p, c_void_p, c_void_p, c_double, c_double]),
     "pp_evolve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPEvolveOpts)]),
     "pp_compact": (c_int32, [c_void_p, POINTER(PPFilter)]),
+    "pp_evolve_batch": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPBatch),
+                                  POINTER(PPEvolveOpts)]),
     "pp_compact_static": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_int64, POINTER(PPFilter),
                                     c_void_p, c_void_p, c_void_p, POINTER(c_int64), c_void_p]),
     "pp_adaptive": (c_int32, [c_void_p, c_int64, c_double]),
