@@ -19,6 +19,10 @@ Arms:
                     of the reference's CPU path (oracle/, "port"), one worker
                     process per host thread, each timing one Trotter layer from
                     the layer-10 state (a bounded sample of the same workload).
+--workload batch256: 256 uneven instances of the 8x8 lattice in one batched pass
+(pp_evolve_batch): depth U{4..24} layers, θ_J, θ_h ~ U[0.05, 0.5], observable a
+random Pauli string of weight 1-4, CoeffTruncation(1e-4), no noise.  One step =
+all 256 instances; the line adds the p50 / p99 instance completion times.
 Multi-GPU (torchrun, N > 1): every rank runs an independent replica of the
 workload (the path does not shard at this size); value = all ranks' terms over
 the slowest rank's time.
@@ -46,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lattice64", "chain20", "graph127"], default="lattice64")
+    ap.add_argument("--workload", choices=["lattice64", "chain20", "graph127", "batch256"], default="lattice64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-workers", type=int, default=0, help="reference arm worker processes (0: all host threads)")
     return ap.parse_args()
@@ -206,6 +210,8 @@ def run_reference(args):
     ctx = mp.get_context("spawn")
     nthreads = args.ref_workers or os.cpu_count() or 1
     q = ctx.Queue()
+    if args.workload == "batch256":
+        return run_reference_batch(args, ctx, q, nthreads)
     reps = args.warmup + args.steps
     procs = [ctx.Process(target=_oracle_layer_sample, args=(args.workload, SNAP_LAYER, reps, q))
              for _ in range(nthreads)]
@@ -232,6 +238,178 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "terms/s", "cores": nthreads, "kind": "port",
                          "sample": f"{w.name}: one Trotter layer ({len(w.layer)} rotations + channel) "
                                    f"from the layer-{SNAP_LAYER} state, per worker process"},
+        "e2e": {"value": value, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+BATCH_COUNT, BATCH_SEED, BATCH_THRESH = 256, 5, 1e-4
+BATCH_CPU_LIMIT = 2_000_000     # CPU sample: layers entered with at most this many live terms
+
+
+def batch_setup():
+    from pauliprop import circuits
+    insts = circuits.batch_instances(count=BATCH_COUNT, seed=BATCH_SEED, thresh=BATCH_THRESH)
+    layer = [(p.z, p.x) for p in insts[0].layer]
+    acol = [0] * 112 + [1] * 64
+    angs = [[w.angles[0], w.angles[-1]] for w in insts]
+    depths = [w.layers for w in insts]
+    obs = [w.observable for w in insts]
+    return insts, layer, acol, angs, depths, obs
+
+
+def _oracle_batch_sample(worker, nworkers, budget_s, q=None):
+    """Worker: the batch's instances worker, worker + nworkers, ... on the CPU oracle,
+    one layer at a time, entering a layer only with at most BATCH_CPU_LIMIT live
+    terms, until budget_s seconds of evolution.  Returns (terms_in, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    import pauliprop as pp
+    insts, layer, acol, angs, depths, obs = batch_setup()
+    f = tuple(pp.compile_filter(pp.CoeffTruncation(BATCH_THRESH)))
+    terms = 0
+    spent = 0.0
+    for i in range(worker, len(insts), nworkers):
+        v = orc.OracleSPV(64, 16, 1 << 22)
+        v.upload([t[0] for t in obs[i]], [t[1] for t in obs[i]], [t[2] for t in obs[i]])
+        ang = [angs[i][a] for a in acol]
+        for _ in range(depths[i]):
+            if len(v) > BATCH_CPU_LIMIT or spent > budget_s:
+                break
+            n0 = len(v)
+            t0 = time.perf_counter()
+            _, ctr = v.evolve(layer, ang, window=1, strict=f, nwin=len(layer))
+            spent += time.perf_counter() - t0
+            terms += n0 + int(ctr[2][:-1].sum())
+        if spent > budget_s:
+            break
+    out = (terms, spent)
+    if q is not None:
+        q.put(out)
+    return out
+
+
+def run_ours_batch(args):
+    import numpy as np
+    import torch
+    ws, rank, local = dist_init("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import pauliprop as pp
+    from pauliprop.batch import tagged_terms
+
+    insts, layer, acol, angs, depths, obs = batch_setup()
+    D = max(depths)
+    gens = layer * D
+    acols = acol * D
+    rend = [d * len(layer) for d in depths]
+    strat = pp.CoeffTruncation(BATCH_THRESH)
+    v = pp.SparsePauliVector(128, 1 << 20, 16)
+    stream = torch.cuda.ExternalStream(v.stream(), device=dev)
+
+    def one_step(profile=False):
+        return pp.evolve_batch(obs, gens, acols, angs, rend, nq=64, truncation=strat, vector=v, profile=profile)
+
+    for _ in range(args.warmup):
+        one_step()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    res = []
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            res.append(one_step())
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t = reduce_max(e0.elapsed_time(e1) * 1e-3, ws, dev)
+    terms_in = res[-1].stats["terms_in"]
+    total_terms = reduce_sum(terms_in * args.steps, ws, dev)
+    value = total_terms / t
+    launches = int(res[-1].stats["launches"])
+    tdone = np.concatenate([r.t_done for r in res])
+    # e2e: the public call from host arrays (upload, evolve, per-instance results back)
+    z, x, c = tagged_terms(obs)
+    te = []
+    for _ in range(args.steps):
+        if ws > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        r = one_step()
+        te.append(time.perf_counter() - t0)
+    t_e2e = reduce_max(sum(te), ws, dev)
+    h2d = z.nbytes + x.nbytes + c.nbytes + len(gens) * (32 + 4) + len(obs) * (2 * 2 * 8 + 8)
+    d2h = len(obs) * (8 + 8 + 8)
+    # profiled pass: merge kernel time for the roofline
+    rp = one_step(profile=True)
+    sp = rp.stats
+    B = BYTES_PER_TERM[2]
+    achieved = B * (sp["merge_in"] + sp["merge_out"]) / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
+    hbm, src = peaks()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ti, dt = _oracle_batch_sample(0, 1, 12.0)
+        cpu = {"value": ti / dt, "unit": "terms/s", "cores": 1, "kind": "port",
+               "sample": f"the batch's instances in order, one layer at a time, layers entered with at most "
+                         f"{BATCH_CPU_LIMIT} live terms, about 12 s of evolution ({ti:.3g} term-rotations); "
+                         f"C restatement of the reference path, 1 thread"}
+    if rank == 0:
+        line = {
+            "metric": "terms/s rotate+merge+clip (batched instances)", "value": value, "unit": "terms/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded instances)",
+            "config": {"workload": f"batch256: {len(obs)} instances of the 8x8 lattice (N=64), depth U{{4..24}} "
+                                   f"layers of 176 rotations, θ_J, θ_h ~ U[0.05, 0.5], observable a random "
+                                   f"weight-1-4 Pauli string, CoeffTruncation({BATCH_THRESH}), no noise",
+                       "instances": len(obs), "rotations": len(gens), "terms_in_per_step": terms_in,
+                       "peak_terms": res[-1].stats["peak"],
+                       "n_final_p50": float(np.percentile(res[-1].n_final, 50)),
+                       "n_final_max": int(res[-1].n_final.max()),
+                       "completion_p50_s": float(np.percentile(tdone, 50)),
+                       "completion_p99_s": float(np.percentile(tdone, 99)),
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "no flush: the live set (up to ~3e8 terms x 40 B) exceeds L2"},
+            "e2e": {"value": total_terms / t_e2e, "unit": "terms/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "kernel": "k_merge<2,0> (merge + reduce-by-key + filter, 40-byte batched terms)",
+                         "peak_source": src, "t_merge_s": sp["t_merge"], "t_rotate_s": sp["t_rotate"],
+                         "t_partition_commit_s": sp["t_partition"]},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    v.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference_batch(args, ctx, q, nthreads):
+    """Reference arm of batch256: the instances split over one worker process per
+    host thread, each evolving its share layer by layer on the C restatement for a
+    bounded time; value = the sum of the workers' term-rotations per second."""
+    budget = 10.0 * args.steps
+    procs = [ctx.Process(target=_oracle_batch_sample, args=(k, nthreads, budget, q)) for k in range(nthreads)]
+    for p in procs:
+        p.start()
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    value = sum(t / s for t, s in res if s > 0)
+    line = {
+        "metric": "terms/s rotate+merge+clip (batched instances)", "value": value, "unit": "terms/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * max(s for _, s in res), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded instances)", "impl": "reference",
+        "config": {"workload": f"batch256 instances, CoeffTruncation({BATCH_THRESH}), layers entered with at "
+                               f"most {BATCH_CPU_LIMIT} live terms", "threads": nthreads},
+        "cpu_baseline": {"value": value, "unit": "terms/s", "cores": nthreads, "kind": "port",
+                         "sample": f"each worker: its share of the instances for about {budget:.0f} s"},
         "e2e": {"value": value, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -403,6 +581,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch256":
+        run_ours_batch(args)
     else:
         run_ours(args)
 

@@ -59,13 +59,14 @@ def split_instances(z, x, c, ninst):
 
 def evolve_batch(observables, generators, acol, angles, rot_end, *, nq, truncation=None,
                  channel=None, channel_every=0, ket=0, keep_finished=False, profile=False,
-                 capacity=None):
+                 capacity=None, vector=None):
     """Evolve len(observables) instances through prefixes of `generators`.
 
     generators: L nq-qubit generators (PauliBasis or (z, x)); acol[r]: angle column
     of rotation r; angles[i][j]: θ of instance i's column j; rot_end[i]: rotations
     instance i runs.  channel=(kind, params, qubits or None) after every
-    `channel_every` rotations (0: after the last rotation)."""
+    `channel_every` rotations (0: after the last rotation).  `vector`: an existing
+    SparsePauliVector(128, ...) to run in (it is overwritten and kept open)."""
     ninst = len(observables)
     if ninst < 1:
         raise ArgumentError("need at least one instance")
@@ -88,7 +89,10 @@ def evolve_batch(observables, generators, acol, angles, rot_end, *, nq, truncati
         gz[r, 0], gx[r, 0] = zz & M64, xx & M64
     z, x, c = tagged_terms(observables)
     n = len(c)
-    v = SparsePauliVector(128, capacity or max(4096, 4 * n), 16)
+    own = vector is None
+    v = SparsePauliVector(128, capacity or max(4096, 4 * n), 16) if own else vector
+    if v.N <= 64:
+        raise ArgumentError("batched instances need a vector with 128-bit words (N > 64)")
     v.upload(z, x, c, sorted=False)
     expect = np.full(ninst, np.nan)
     t_done = np.zeros(ninst)
@@ -125,7 +129,7 @@ def evolve_batch(observables, generators, acol, angles, rot_end, *, nq, truncati
     opts.profile = 1 if profile else 0
     check(lib.pp_evolve_batch(v._h, _ptr(gz), _ptr(gx), L, byref(b), byref(opts)))
     stats = {name: float(st[i]) for name, i in _lib.STAT.items()}
-    if not keep_finished:
+    if not keep_finished and own:
         v.close()
         v = None
     return BatchResult(expect, t_done, n_final, stats, v)
