@@ -150,6 +150,55 @@ typedef struct {
  * vectors evolve one at a time). */
 int pp_evolve_batch(pp_spv *h, const void *gz, const void *gx, int64_t L, const pp_batch *b,
                     const pp_evolve_opts *opts);
+/* ---- Learned truncation.  No counterpart in the reference (which truncates by
+ * coefficient and weight only).  A 16 -> 64 -> 64 -> 1 GELU network predicts
+ * log10 |contribution of a term to the final expectation value| from 16 term
+ * features; a budget truncation keeps the `budget` terms of largest prediction
+ * (ties: the smaller (z, x) key).  Matrices are BF16 on the tensor cores with
+ * FP32 accumulation; parameters are an FP32 vector of PP_MLP_NPARAM values laid
+ * out W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3. */
+#define PP_MLP_NPARAM 5313
+typedef struct pp_mlp pp_mlp;
+
+/* Position of a vector in its circuit and the lattice geometry the features use
+ * (N <= 64 qubits; qubit q is bit q-1). */
+typedef struct {
+    int32_t nq;                   /* qubits */
+    int32_t pad;
+    uint64_t nbr[64];             /* neighbour mask of each qubit */
+    uint64_t light_cone;          /* qubits in the remaining circuit's light cone */
+    uint64_t boundary;            /* qubits on the lattice boundary */
+    uint8_t row[64], col[64];     /* lattice coordinates of each qubit */
+    float layer_frac;             /* layers done / total layers */
+    float remaining_frac;         /* layers to go / total layers */
+    float theta_j, theta_h;       /* the circuit's angles */
+} pp_feature_ctx;
+
+int pp_mlp_create(pp_mlp **out);
+int pp_mlp_destroy(pp_mlp *m);
+/* Sets / reads the FP32 parameters (host or device pointers); set resets Adam. */
+int pp_mlp_set_params(pp_mlp *m, const float *params);
+int pp_mlp_get_params(pp_mlp *m, float *params);
+/* out[i] = network(feat[i][0..15]) for i < n (host or device pointers). */
+int pp_mlp_forward(pp_mlp *m, const float *feat, int64_t n, float *out);
+/* Gradient of mean_i (network(feat[i]) - target[i])^2 over all n rows with respect to
+ * the parameters (PP_MLP_NPARAM floats) and the loss. */
+int pp_mlp_grad(pp_mlp *m, const float *feat, const float *target, int64_t n, float *grad, float *loss);
+/* Copies a training set (n rows of 16 features and a target) to the device. */
+int pp_mlp_load_data(pp_mlp *m, const float *feat, const float *target, int64_t n);
+/* `steps` Adam steps (lr; betas 0.9, 0.999) on minibatches of `batch` rows drawn
+ * without replacement per epoch (seeded shuffle); loss_out[steps] gets each step's
+ * minibatch loss (nullable). */
+int pp_mlp_train(pp_mlp *m, int64_t steps, int64_t batch, float lr, uint64_t seed, float *loss_out);
+/* The 16 features of each live term (n x 16 FP32, host or device; at most cap rows);
+ * *n_out = live count. */
+int pp_features(pp_spv *h, const pp_feature_ctx *ctx, float *out, int64_t cap, int64_t *n_out);
+/* Budget truncation: when more than `budget` terms are live, keeps exactly the
+ * `budget` of largest network output (computed from the live terms in one fused
+ * pass), in key order.  *cut_score: the smallest kept output (-inf when nothing
+ * was dropped). */
+int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *ctx, int64_t budget, float *cut_score);
+
 /* coeff_clip! / weight_clip! / x_weight_clip! / majorana_weight_clip! /
  * weight_damped_clip! / x_weight_damped_clip! and the compilable truncate!
  * (spv_evolve.jl:13-26, 59-65) -> _compact_spv! (spv_kernels.jl:395-408). */

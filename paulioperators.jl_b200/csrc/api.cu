@@ -21,6 +21,7 @@
 #include "../../include/pauliprop.h"
 #include "kernels_general.cuh"
 #include "kernels_batch.cuh"
+#include "kernels_learned.cuh"
 
 using namespace pp;
 
@@ -1313,4 +1314,318 @@ extern "C" int pp_evolve_batch(pp_spv *h, const void *gz, const void *gx, int64_
         }
     }
     return r;
+}
+
+// ------------------------------------------------------------------ learned truncation
+static_assert(sizeof(pp_feature_ctx) == sizeof(FeatCtx), "pp_feature_ctx mirrors FeatCtx");
+static_assert(PP_MLP_NPARAM == MLP_NPARAM, "parameter count");
+
+struct pp_mlp {
+    int dev = 0, nsm = 148;
+    cudaStream_t stream = nullptr;
+    MlpDev *W = nullptr;
+    float *p = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;   // master params, Adam moments, grad (+loss)
+    float *gpart = nullptr;
+    float *feat = nullptr, *target = nullptr, *out = nullptr;
+    long long ndata = 0, data_cap = 0, out_cap = 0;
+    int *idx = nullptr;
+    long long idx_cap = 0;
+    float *loss_log = nullptr;
+    long long loss_cap = 0;
+    FeatCtx *ctx = nullptr;
+    int *err = nullptr;
+    long long step = 0;
+    // selection workspaces (used with a pp_spv's stream)
+    float *score = nullptr;
+    long long score_cap = 0;
+    SelectState *sel = nullptr;
+    int *cgt = nullptr, *ceq = nullptr, *tie_off = nullptr, *out_off = nullptr;
+    long long *total = nullptr;
+    long long tiles_cap = 0;
+};
+
+#define MCU(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? PP_OUT_OF_MEMORY : PP_DEVICE_ERROR, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+template <typename T>
+static int malloc_n(T **p, long long n) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    MCU(cudaMalloc((void **)p, (size_t)std::max(1ll, n) * sizeof(T)));
+    return PP_OK;
+}
+
+static int mlp_check(pp_mlp *m) {
+    MCU(cudaStreamSynchronize(m->stream));
+    int e = 0;
+    MCU(cudaMemcpy(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(m->err, 0, sizeof(int));
+        return fail(e & ERR_TIMEOUT ? PP_TIMEOUT : PP_ERROR_EXCEPTION, "learned-truncation kernel error flag set");
+    }
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_create(pp_mlp **out) {
+    if (!out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    pp_mlp *m = new pp_mlp();
+    auto bail = [&](int r) { pp_mlp_destroy(m); return r; };
+    int r;
+    if (cudaGetDevice(&m->dev) != cudaSuccess) return bail(fail(PP_DEVICE_ERROR, "no CUDA device"));
+    cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, m->dev);
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(PP_DEVICE_ERROR, "stream"));
+    if ((r = malloc_n(&m->W, 1)) || (r = malloc_n(&m->p, MLP_NPARAM)) || (r = malloc_n(&m->m, MLP_NPARAM)) ||
+        (r = malloc_n(&m->v, MLP_NPARAM)) || (r = malloc_n(&m->g, MLP_NPARAM + 1)) ||
+        (r = malloc_n(&m->gpart, (long long)m->nsm * (MLP_NPARAM + 1))) || (r = malloc_n(&m->ctx, 1)) ||
+        (r = malloc_n(&m->err, 1)) || (r = malloc_n(&m->sel, 1)) || (r = malloc_n(&m->total, 1)))
+        return bail(r);
+    cudaMemset(m->W, 0, sizeof(MlpDev));
+    cudaMemset(m->p, 0, MLP_NPARAM * 4);
+    cudaMemset(m->m, 0, MLP_NPARAM * 4);
+    cudaMemset(m->v, 0, MLP_NPARAM * 4);
+    cudaMemset(m->err, 0, 4);
+    if (cudaFuncSetAttribute(k_mlp_fwd<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_FWD_SMEM) ||
+        cudaFuncSetAttribute(k_mlp_fwd<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_FWD_SMEM) ||
+        cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_GRAD_SMEM))
+        return bail(fail(PP_DEVICE_ERROR, "cudaFuncSetAttribute (shared memory)"));
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(PP_DEVICE_ERROR, "device"));
+    *out = m;
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_destroy(pp_mlp *m) {
+    if (!m) return PP_OK;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    void *ptrs[] = {m->W, m->p, m->m, m->v, m->g, m->gpart, m->feat, m->target, m->out, m->idx, m->loss_log,
+                    m->ctx, m->err, m->score, m->sel, m->cgt, m->ceq, m->tie_off, m->out_off, m->total};
+    for (void *q : ptrs) if (q) cudaFree(q);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_set_params(pp_mlp *m, const float *params) {
+    if (!m || !params) return fail(PP_ARGUMENT_ERROR, "null argument");
+    MCU(cudaMemcpyAsync(m->p, params, MLP_NPARAM * 4, cudaMemcpyDefault, m->stream));
+    MCU(cudaMemsetAsync(m->m, 0, MLP_NPARAM * 4, m->stream));
+    MCU(cudaMemsetAsync(m->v, 0, MLP_NPARAM * 4, m->stream));
+    k_mlp_set<<<(MLP_NPARAM + 255) / 256, 256, 0, m->stream>>>(m->p, m->W);
+    m->step = 0;
+    return mlp_check(m);
+}
+
+extern "C" int pp_mlp_get_params(pp_mlp *m, float *params) {
+    if (!m || !params) return fail(PP_ARGUMENT_ERROR, "null argument");
+    MCU(cudaMemcpyAsync(params, m->p, MLP_NPARAM * 4, cudaMemcpyDefault, m->stream));
+    return mlp_check(m);
+}
+
+static int mlp_stage(pp_mlp *m, const float *feat, const float *target, long long n) {
+    if (n > m->data_cap) {
+        TRY(malloc_n(&m->feat, n * MLP_F));
+        TRY(malloc_n(&m->target, n));
+        m->data_cap = n;
+    }
+    if (n > 0) {
+        MCU(cudaMemcpyAsync(m->feat, feat, n * MLP_F * 4, cudaMemcpyDefault, m->stream));
+        if (target) MCU(cudaMemcpyAsync(m->target, target, n * 4, cudaMemcpyDefault, m->stream));
+    }
+    m->ndata = n;
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_forward(pp_mlp *m, const float *feat, int64_t n, float *out) {
+    if (!m || n < 0 || (n > 0 && (!feat || !out))) return fail(PP_ARGUMENT_ERROR, "bad argument");
+    TRY(mlp_stage(m, feat, nullptr, n));
+    if (n > m->out_cap) {
+        TRY(malloc_n(&m->out, n));
+        m->out_cap = n;
+    }
+    if (n == 0) return PP_OK;
+    const long long tiles = (n + MLP_ROWS - 1) / MLP_ROWS;
+    const int grid = (int)std::min<long long>(tiles, 4ll * m->nsm);
+    k_mlp_fwd<0><<<grid, MLP_ROWS, MLP_FWD_SMEM, m->stream>>>(m->feat, nullptr, nullptr, nullptr, n, nullptr, m->W,
+                                                              m->out, nullptr, m->err);
+    MCU(cudaGetLastError());
+    MCU(cudaMemcpyAsync(out, m->out, n * 4, cudaMemcpyDefault, m->stream));
+    return mlp_check(m);
+}
+
+// One gradient of mean((y - t)^2) over idx[0, B) of the staged data into m->g.
+static int mlp_grad_launch(pp_mlp *m, const int *idx, long long B) {
+    const long long tiles = (B + MLP_ROWS - 1) / MLP_ROWS;
+    const int grid = (int)std::min<long long>(tiles, m->nsm);
+    k_mlp_grad<<<grid, MLP_ROWS, MLP_GRAD_SMEM, m->stream>>>(m->feat, m->target, idx, B, m->W, m->gpart, m->err);
+    k_mlp_reduce<<<(MLP_NPARAM + 1 + 255) / 256, 256, 0, m->stream>>>(m->gpart, grid, m->g);
+    MCU(cudaGetLastError());
+    return PP_OK;
+}
+
+static int mlp_ensure_idx(pp_mlp *m, long long n) {
+    if (n > m->idx_cap) {
+        TRY(malloc_n(&m->idx, n));
+        m->idx_cap = n;
+    }
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_grad(pp_mlp *m, const float *feat, const float *target, int64_t n, float *grad, float *loss) {
+    if (!m || n <= 0 || !feat || !target || !grad) return fail(PP_ARGUMENT_ERROR, "bad argument");
+    if (n > (1ll << 31) - 1) return fail(PP_ARGUMENT_ERROR, "n too large");
+    TRY(mlp_stage(m, feat, target, n));
+    TRY(mlp_ensure_idx(m, n));
+    std::vector<int> id((size_t)n);
+    for (long long i = 0; i < n; ++i) id[i] = (int)i;
+    MCU(cudaMemcpyAsync(m->idx, id.data(), n * 4, cudaMemcpyHostToDevice, m->stream));
+    TRY(mlp_grad_launch(m, m->idx, n));
+    std::vector<float> g(MLP_NPARAM + 1);
+    MCU(cudaMemcpyAsync(g.data(), m->g, (MLP_NPARAM + 1) * 4, cudaMemcpyDeviceToHost, m->stream));
+    TRY(mlp_check(m));
+    memcpy(grad, g.data(), MLP_NPARAM * 4);
+    if (loss) *loss = g[MLP_NPARAM] / (float)n;
+    return PP_OK;
+}
+
+extern "C" int pp_mlp_load_data(pp_mlp *m, const float *feat, const float *target, int64_t n) {
+    if (!m || n <= 0 || !feat || !target) return fail(PP_ARGUMENT_ERROR, "bad argument");
+    if (n > (1ll << 31) - 1) return fail(PP_ARGUMENT_ERROR, "n too large");
+    TRY(mlp_stage(m, feat, target, n));
+    return mlp_check(m);
+}
+
+static inline uint64_t splitmix64(uint64_t *s) {
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+extern "C" int pp_mlp_train(pp_mlp *m, int64_t steps, int64_t batch, float lr, uint64_t seed, float *loss_out) {
+    if (!m || steps < 0 || batch < 1 || !(lr > 0.0f)) return fail(PP_ARGUMENT_ERROR, "bad argument");
+    const long long nd = m->ndata;
+    if (nd < 1) return fail(PP_ARGUMENT_ERROR, "no training data loaded (pp_mlp_load_data)");
+    batch = std::min<long long>(batch, nd);
+    TRY(mlp_ensure_idx(m, nd));
+    if (steps > m->loss_cap) {
+        TRY(malloc_n(&m->loss_log, steps));
+        m->loss_cap = steps;
+    }
+    std::vector<int> perm((size_t)nd);
+    for (long long i = 0; i < nd; ++i) perm[i] = (int)i;
+    uint64_t st = seed;
+    long long pos = nd;   // forces a shuffle first
+    for (long long s = 0; s < steps; ++s) {
+        if (pos + batch > nd) {
+            for (long long i = nd - 1; i > 0; --i) std::swap(perm[i], perm[splitmix64(&st) % (uint64_t)(i + 1)]);
+            MCU(cudaMemcpyAsync(m->idx, perm.data(), nd * 4, cudaMemcpyHostToDevice, m->stream));
+            MCU(cudaStreamSynchronize(m->stream));
+            pos = 0;
+        }
+        TRY(mlp_grad_launch(m, m->idx + pos, batch));
+        m->step += 1;
+        k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, m->stream>>>(m->p, m->m, m->v, m->g, (int)m->step, lr, m->W,
+                                                                    m->loss_log + s, batch);
+        pos += batch;
+    }
+    MCU(cudaGetLastError());
+    if (loss_out && steps > 0) MCU(cudaMemcpyAsync(loss_out, m->loss_log, steps * 4, cudaMemcpyDeviceToHost, m->stream));
+    return mlp_check(m);
+}
+
+extern "C" int pp_features(pp_spv *h, const pp_feature_ctx *ctx, float *out, int64_t cap, int64_t *n_out) {
+    if (!h || !ctx || !n_out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    if (h->NW != 1) return fail(PP_ARGUMENT_ERROR, "term features need N <= 64");
+    DevState st;
+    TRY(read_state(h, &st));
+    *n_out = st.n;
+    const long long n = std::min<long long>(st.n, std::max<int64_t>(cap, 0));
+    if (n == 0) return PP_OK;
+    if (!out) return fail(PP_ARGUMENT_ERROR, "null output");
+    FeatCtx *dctx = nullptr;
+    float *dout = nullptr;
+    CU(cudaMalloc((void **)&dctx, sizeof(FeatCtx)));
+    cudaError_t e = cudaMalloc((void **)&dout, (size_t)n * MLP_F * 4);
+    if (e != cudaSuccess) { cudaFree(dctx); return fail(PP_OUT_OF_MEMORY, "features buffer"); }
+    cudaMemcpyAsync(dctx, ctx, sizeof(FeatCtx), cudaMemcpyHostToDevice, h->stream);
+    k_features<<<h->nsm * 8, 256, 0, h->stream>>>(h->z[st.cur], h->x[st.cur], h->c[st.cur], n, dctx, dout);
+    e = cudaMemcpyAsync(out, dout, (size_t)n * MLP_F * 4, cudaMemcpyDefault, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(dctx);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, cudaGetErrorString(e));
+    return sync_check(h);
+}
+
+extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *ctx, int64_t budget,
+                                   float *cut_score) {
+    if (!h || !m || !ctx || budget < 0) return fail(PP_ARGUMENT_ERROR, "bad argument");
+    if (h->NW != 1) return fail(PP_ARGUMENT_ERROR, "learned truncation needs N <= 64");
+    DevState st;
+    TRY(read_state(h, &st));
+    if (cut_score) *cut_score = -INFINITY;
+    const long long n = st.n;
+    if (n <= budget) return PP_OK;
+    MCU(cudaStreamSynchronize(m->stream));   // the network's last update is visible to h's stream
+    if (n > m->score_cap) {
+        TRY(malloc_n(&m->score, n));
+        m->score_cap = n;
+    }
+    const long long ntiles = (n + SL_TILE - 1) / SL_TILE;
+    if (ntiles > m->tiles_cap) {
+        TRY(malloc_n(&m->cgt, ntiles));
+        TRY(malloc_n(&m->ceq, ntiles));
+        TRY(malloc_n(&m->tie_off, ntiles));
+        TRY(malloc_n(&m->out_off, ntiles));
+        m->tiles_cap = ntiles;
+    }
+    cudaStream_t s = h->stream;
+    SelectState s0;
+    memset(&s0, 0, sizeof s0);
+    s0.remaining = budget;
+    CU(cudaMemcpyAsync(m->ctx, ctx, sizeof(FeatCtx), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(m->sel, &s0, sizeof s0, cudaMemcpyHostToDevice, s));
+    const int cur = st.cur;
+    const long long rtiles = (n + MLP_ROWS - 1) / MLP_ROWS;
+    k_mlp_fwd<1><<<(int)std::min<long long>(rtiles, 4ll * m->nsm), MLP_ROWS, MLP_FWD_SMEM, s>>>(
+        nullptr, h->z[cur], h->x[cur], h->c[cur], n, m->ctx, m->W, m->score, m->sel, m->err);
+    k_sel_pick<<<1, 32, 0, s>>>(m->sel, 24);
+    for (int shift = 16; shift >= 0; shift -= 8) {
+        k_sel_hist<<<h->nsm * 4, 256, 0, s>>>(m->score, n, m->sel, shift);
+        k_sel_pick<<<1, 32, 0, s>>>(m->sel, shift);
+    }
+    const int g = (int)std::min<long long>(ntiles, 8ll * h->nsm);
+    k_sel_count<<<g, SL_THREADS, 0, s>>>(m->score, n, m->sel, m->cgt, m->ceq);
+    k_sel_scan<<<1, 1024, 0, s>>>(ntiles, m->sel, m->cgt, m->ceq, m->tie_off, m->out_off, m->total);
+    k_sel_write<<<g, SL_THREADS, 0, s>>>(m->score, n, m->sel, m->tie_off, m->out_off, h->z[cur], h->x[cur], h->c[cur],
+                                         h->z[cur ^ 1], h->x[cur ^ 1], h->c[cur ^ 1]);
+    CU(cudaGetLastError());
+    long long kept = 0;
+    SelectState sf;
+    CU(cudaMemcpyAsync(&kept, m->total, sizeof kept, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&sf, m->sel, sizeof sf, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    int e = 0;
+    CU(cudaMemcpy(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(m->err, 0, sizeof(int));
+        return fail(PP_TIMEOUT, "learned truncation: a tensor-core wait timed out");
+    }
+    if (kept != budget) return fail(PP_ERROR_EXCEPTION, "learned truncation kept a count other than the budget");
+    TRY(read_state(h, &st));
+    st.n = kept;
+    st.cur ^= 1;
+    TRY(write_state(h, &st));
+    if (cut_score) {
+        const uint32_t k = sf.prefix;
+        const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+        float f;
+        memcpy(&f, &u, 4);
+        *cut_score = f;
+    }
+    return PP_OK;
 }

@@ -21,6 +21,7 @@ from .spv import (SparsePauliVector, WindowCounters, bit_flip_channel, bit_flip_
                   phase_flip_channel_, power_table, truncate_, weight_clip_,
                   weight_damped_clip_, x_weight_clip_, x_weight_damped_clip_)
 from .batch import BatchResult, evolve_batch, split_instances, tagged_terms
+from .learned import MLP, features, lattice_feature_ctx, learned_truncate_
 from . import circuits
 
 __all__ = [n for n in dir() if not n.startswith("_")]

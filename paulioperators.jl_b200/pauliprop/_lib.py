@@ -8,7 +8,8 @@ device every compute entry point returns PP_DEVICE_ERROR, which is raised as
 """
 import ctypes
 import os
-from ctypes import POINTER, Structure, c_char_p, c_double, c_int32, c_int64, c_void_p
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_int64, c_uint8, c_uint64,
+                    c_void_p)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PAULIPROP_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libpauliprop.so")
@@ -74,6 +75,13 @@ class PPBatch(Structure):
                 ("expect_out", c_void_p), ("t_done", c_void_p), ("n_final", c_void_p)]
 
 
+class PPFeatureCtx(Structure):
+    _fields_ = [("nq", c_int32), ("pad", c_int32), ("nbr", c_uint64 * 64), ("light_cone", c_uint64),
+                ("boundary", c_uint64), ("row", c_uint8 * 64), ("col", c_uint8 * 64),
+                ("layer_frac", c_float), ("remaining_frac", c_float), ("theta_j", c_float), ("theta_h", c_float)]
+
+
+PP_MLP_NPARAM = 5313
 PP_STATS_LEN = 16
 STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
         "t_rotate": 6, "t_merge": 7, "launches": 8, "t_partition": 9}
@@ -101,6 +109,16 @@ SIGNATURES = {
     "pp_stream": (c_int32, [c_void_p, POINTER(c_void_p)]),
     "pp_device_bytes": (c_int32, [c_void_p, POINTER(c_int64)]),
     "pp_power_table": (c_int32, [c_double, c_int32, c_void_p]),
+    "pp_mlp_create": (c_int32, [POINTER(c_void_p)]),
+    "pp_mlp_destroy": (c_int32, [c_void_p]),
+    "pp_mlp_set_params": (c_int32, [c_void_p, c_void_p]),
+    "pp_mlp_get_params": (c_int32, [c_void_p, c_void_p]),
+    "pp_mlp_forward": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "pp_mlp_grad": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, POINTER(c_float)]),
+    "pp_mlp_load_data": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64]),
+    "pp_mlp_train": (c_int32, [c_void_p, c_int64, c_int64, c_float, c_uint64, c_void_p]),
+    "pp_features": (c_int32, [c_void_p, POINTER(PPFeatureCtx), c_void_p, c_int64, POINTER(c_int64)]),
+    "pp_learned_truncate": (c_int32, [c_void_p, c_void_p, POINTER(PPFeatureCtx), c_int64, POINTER(c_float)]),
     "pp_last_error": (c_char_p, []),
 }
 
