@@ -23,6 +23,13 @@ Arms:
 (pp_evolve_batch): depth U{4..24} layers, θ_J, θ_h ~ U[0.05, 0.5], observable a
 random Pauli string of weight 1-4, CoeffTruncation(1e-4), no noise.  One step =
 all 256 instances; the line adds the p50 / p99 instance completion times.
+--workload learned: the learned-truncation protocol on the 8x8-lattice circuit
+(20 layers, depolarizing 1e-3, weight cap 12): the network is trained on labels
+the engine generates (sampled terms propagated exactly through the remaining
+layers), then on held-out angle draws the GPU time to reach |<O> - <O>_ref| <=
+1e-3 is measured for budget truncation by the network and for plain threshold
+truncation; the reference run is plain threshold 1e-6 (1e-7 exceeds 2^31 live
+terms on this circuit).  value = median learned time (lower is better).
 Multi-GPU (torchrun, N > 1): every rank runs an independent replica of the
 workload (the path does not shard at this size); value = all ranks' terms over
 the slowest rank's time.
@@ -50,7 +57,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lattice64", "chain20", "graph127", "batch256"], default="lattice64")
+    ap.add_argument("--workload", choices=["lattice64", "chain20", "graph127", "batch256", "learned"],
+                    default="lattice64")
+    ap.add_argument("--learned-scale", choices=["full", "small"], default="full",
+                    help="learned: 'small' is a quick run of the same protocol on fewer draws and samples")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-workers", type=int, default=0, help="reference arm worker processes (0: all host threads)")
     return ap.parse_args()
@@ -212,6 +222,10 @@ def run_reference(args):
     q = ctx.Queue()
     if args.workload == "batch256":
         return run_reference_batch(args, ctx, q, nthreads)
+    if args.workload == "learned":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned truncation "
+                          "(its plain threshold path is the plain arm of this workload)"}), flush=True)
+        return
     reps = args.warmup + args.steps
     procs = [ctx.Process(target=_oracle_layer_sample, args=(args.workload, SNAP_LAYER, reps, q))
              for _ in range(nthreads)]
@@ -415,6 +429,80 @@ def run_reference_batch(args, ctx, q, nthreads):
     print(json.dumps(line), flush=True)
 
 
+LEARN = {
+    "full": dict(n_train=8, n_test=3, sample_layers=(6, 10, 14), per_layer=6000, train_steps=4000, batch=8192,
+                 budgets=(1e6, 2e6, 5e6, 1e7, 2e7, 4e7), plain=(1e-5, 6e-6, 4e-6, 3e-6, 2e-6, 1.5e-6)),
+    "small": dict(n_train=2, n_test=1, sample_layers=(8, 12), per_layer=2000, train_steps=800, batch=4096,
+                  budgets=(2e6, 1e7), plain=(1e-5, 3e-6)),
+}
+LEARN_T_REF, LEARN_T_BASE, LEARN_LABEL_T, LEARN_TOL = 1e-6, 1e-6, 1e-7, 1e-3
+LEARN_AUDIT = dict(layers=(5, 11), sample=1024, bound=2.5e-4, label_thresh=1e-7)
+
+
+def run_learned_bench(args):
+    import numpy as np
+    import pauliprop as pp
+    from pauliprop import learned as L
+    cfg = LEARN[args.learned_scale]
+    lat = L.Lattice(8, 8, 20)
+    train = L.angle_draws(cfg["n_train"], seed=41)
+    test = L.angle_draws(cfg["n_test"], seed=42)
+    t0 = time.perf_counter()
+    X, T, lab = L.training_set(lat, train, cfg["sample_layers"], cfg["per_layer"], LEARN_T_BASE, LEARN_LABEL_T)
+    t_data = time.perf_counter() - t0
+    # the last training draw's samples validate the fit
+    nval = len(T) // cfg["n_train"] if cfg["n_train"] > 1 else len(T) // 5
+    mlp = pp.MLP(L.init_params(0))
+    mlp.load_data(X[:-nval], T[:-nval])
+    t1 = time.perf_counter()
+    losses = mlp.train(cfg["train_steps"], batch=cfg["batch"], lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t1
+    yv = mlp.forward(X[-nval:])
+    r2 = 1.0 - float(np.mean((yv - T[-nval:]) ** 2) / max(1e-30, np.var(T[-nval:])))
+    rows = []
+    for draw in test:
+        e_ref, t_ref, peak_ref = L.run_plain(lat, draw, LEARN_T_REF)
+        plain = []
+        for t in cfg["plain"]:
+            e, dt, pk = L.run_plain(lat, draw, t)
+            plain.append({"thresh": t, "err": abs(e - e_ref), "s": dt, "peak": pk})
+        learned, coeff = [], []
+        for B in cfg["budgets"]:
+            e, dt, pk, au = L.run_learned(lat, draw, mlp, int(B), LEARN_T_BASE, audit=LEARN_AUDIT)
+            learned.append({"budget": B, "err": abs(e - e_ref), "s": dt, "peak": pk, "reverted": au["reverted"],
+                            "audits": au["audits"]})
+            e2, dt2, pk2, _ = L.run_learned(lat, draw, None, int(B), LEARN_T_BASE)
+            coeff.append({"budget": B, "err": abs(e2 - e_ref), "s": dt2, "peak": pk2})
+        rows.append({"draw": draw, "ref": {"expect": e_ref, "s": t_ref, "peak": peak_ref}, "plain": plain,
+                     "learned": learned, "coeff_budget": coeff,
+                     "t_learned": L.time_to_error([(r["err"], r["s"]) for r in learned], LEARN_TOL),
+                     "t_plain": L.time_to_error([(r["err"], r["s"]) for r in plain], LEARN_TOL),
+                     "t_coeff_budget": L.time_to_error([(r["err"], r["s"]) for r in coeff], LEARN_TOL)})
+    med = lambda k: (statistics.median([r[k] for r in rows if r[k] is not None])
+                     if any(r[k] is not None for r in rows) else None)
+    tl, tp = med("t_learned"), med("t_plain")
+    line = {
+        "metric": "time to |Δ⟨O⟩|≤1e-3 learned vs plain truncation", "value": tl, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "steps": 1, "warmup": 0, "dtype": "f64 (terms) / bf16 (network)",
+        "data": "synthetic (seeded angle draws; labels generated by the engine)", "vs_baseline": None,
+        "scaling": "weak",
+        "config": {"workload": "learned truncation on the 8x8 lattice circuit (N=64, 20 layers of RZZ(θ_J) on 112 "
+                               "edges + RX(θ_h) on 64 sites, depolarizing 1e-3, weight cap 12); θ_J ~ U[0.22,0.32], "
+                               "θ_h ~ U[0.18,0.28]",
+                   "reference_threshold": LEARN_T_REF, "base_threshold": LEARN_T_BASE,
+                   "label_threshold": LEARN_LABEL_T, "tolerance": LEARN_TOL, "scale": args.learned_scale,
+                   "train_draws": len(train), "test_draws": len(test), "samples": int(len(T)),
+                   "validation_r2": r2, "data_seconds": t_data, "train_seconds": t_train,
+                   "train_tflops": 6 * 5313 * cfg["train_steps"] * cfg["batch"] / t_train / 1e12,
+                   "loss_first_last": [float(losses[:10].mean()), float(losses[-10:].mean())],
+                   "audit": LEARN_AUDIT},
+        "plain_time_s": tp, "coeff_budget_time_s": med("t_coeff_budget"),
+        "learned_over_plain": (tl / tp) if (tl and tp) else None,
+        "draws": rows,
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args):
     import numpy as np
@@ -583,6 +671,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch256":
         run_ours_batch(args)
+    elif args.workload == "learned":
+        run_learned_bench(args)
     else:
         run_ours(args)
 

@@ -193,11 +193,30 @@ int pp_mlp_train(pp_mlp *m, int64_t steps, int64_t batch, float lr, uint64_t see
 /* The 16 features of each live term (n x 16 FP32, host or device; at most cap rows);
  * *n_out = live count. */
 int pp_features(pp_spv *h, const pp_feature_ctx *ctx, float *out, int64_t cap, int64_t *n_out);
+/* Stratified random sample of the live terms (N <= 64), for building training
+ * sets: nbins equal-width bins of log10 |c| over [lg_lo, lg_hi) (outside values
+ * fall into the end bins), about 0.9 per_bin terms from each bin (all of a bin
+ * with fewer), chosen by a hash of (seed, index); at most cap rows, in no
+ * particular order. */
+int pp_sample_terms(pp_spv *h, int32_t nbins, double lg_lo, double lg_hi, int64_t per_bin, uint64_t seed,
+                    void *z, void *x, double *c, int64_t cap, int64_t *n_out);
+/* Uniform sample of the terms a budget truncation drops (for auditing the cut):
+ * up to cap terms (word 0 of z / x, coefficient), each dropped term taken with
+ * probability 0.9 cap / n_dropped by a hash of (seed, its index). */
+typedef struct {
+    int64_t cap;                  /* in: buffer rows (0: no sample) */
+    uint64_t seed;                /* in */
+    void *z, *x;                  /* out: host or device, cap words each */
+    double *c;                    /* out: cap coefficients */
+    int64_t n;                    /* out: rows written */
+    int64_t n_dropped;            /* out: terms the cut dropped */
+} pp_drop_sample;
 /* Budget truncation: when more than `budget` terms are live, keeps exactly the
  * `budget` of largest network output (computed from the live terms in one fused
  * pass), in key order.  *cut_score: the smallest kept output (-inf when nothing
- * was dropped). */
-int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *ctx, int64_t budget, float *cut_score);
+ * was dropped).  sample: nullable. */
+int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *ctx, int64_t budget, float *cut_score,
+                        pp_drop_sample *sample);
 
 /* coeff_clip! / weight_clip! / x_weight_clip! / majorana_weight_clip! /
  * weight_damped_clip! / x_weight_damped_clip! and the compilable truncate!

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/pauliprop.h"
@@ -81,6 +82,7 @@ struct pp_spv {
     long long gens_h_cap = 0;
     int occA1 = 1, occA3 = 1, occB = 1, occG = 1;
     long long bytes = 0;
+    std::unordered_map<void *, size_t> sizes;   // bytes of each live device allocation
     long long acap_logical_init = 16;
     long long buf_gen = 0;                 // bumped by every (re)allocation
     int *sphys = nullptr, *soff = nullptr;   // live segment table (physical base, dense start)
@@ -103,17 +105,34 @@ struct pp_spv {
 };
 
 // ------------------------------------------------------------------ helpers
+static void dfree(pp_spv *h, void *p) {
+    if (!p) return;
+    auto it = h->sizes.find(p);
+    if (it != h->sizes.end()) {
+        h->bytes -= (long long)it->second;
+        h->sizes.erase(it);
+    }
+    cudaFree(p);
+}
+
+// (Re)allocates *p for count elements.  The new buffer is allocated before the
+// old one is freed, so a failure leaves *p (and everything sized from it) as it
+// was: callers update their capacity fields only after every allocation of a
+// growth step succeeded, and the handle stays usable after an out-of-memory.
 template <typename T>
 static int dalloc(pp_spv *h, T **p, long long count) {
-    if (*p) { cudaFree(*p); *p = nullptr; }
     if (count <= 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, (size_t)count * sizeof(T));
+    void *q = nullptr;
+    const size_t b = (size_t)count * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, b);
     if (e != cudaSuccess) {
-        *p = nullptr;
         cudaGetLastError();
         return fail(PP_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
-    h->bytes += (long long)count * sizeof(T);
+    dfree(h, *p);
+    *p = (T *)q;
+    h->sizes[q] = b;
+    h->bytes += (long long)b;
     h->buf_gen++;
     return PP_OK;
 }
@@ -204,27 +223,46 @@ static int grow_live(pp_spv *h, long long need) {
         TRY(ensure_dense(h));
         TRY(read_state(h, &st));
     }
-    u64 *nz = nullptr, *nx = nullptr;
-    double *nc = nullptr;
-    long long saved = h->bytes;
-    TRY(dalloc(h, &nz, newcap * h->NW));
-    TRY(dalloc(h, &nx, newcap * h->NW));
-    TRY(dalloc(h, &nc, newcap));
-    if (have && st.n > 0) {
-        CU(cudaMemcpyAsync(nz, h->z[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
-        CU(cudaMemcpyAsync(nx, h->x[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
-        CU(cudaMemcpyAsync(nc, h->c[st.cur], st.n * 8, cudaMemcpyDeviceToDevice, h->stream));
+    // refuse a growth that would leave less than 4 GiB of device memory free
+    {
+        size_t freeb = 0, totalb = 0;
+        if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) {
+            const double want = (double)newcap * (2.0 * (2 * h->NW * 8 + 8) + 12.0 + 4.0 * TAU_MAX * 2.0 / SEG);
+            if (want + 4.0 * (1ull << 30) > (double)freeb)
+                return fail(PP_OUT_OF_MEMORY, "growing to " + std::to_string(newcap) +
+                                                  " terms would leave less than 4 GiB of device memory free");
+        }
     }
-    CU(cudaStreamSynchronize(h->stream));
+    // both new term sets first; on failure the handle is unchanged
+    u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
+    double *nc[2] = {nullptr, nullptr};
+    auto drop = [&]() {
+        for (int s = 0; s < 2; ++s) { dfree(h, nz[s]); dfree(h, nx[s]); dfree(h, nc[s]); }
+    };
     for (int s = 0; s < 2; ++s) {
-        if (h->z[s]) { cudaFree(h->z[s]); cudaFree(h->x[s]); cudaFree(h->c[s]); }
-        h->z[s] = nullptr; h->x[s] = nullptr; h->c[s] = nullptr;
+        int r = dalloc(h, &nz[s], newcap * h->NW);
+        if (!r) r = dalloc(h, &nx[s], newcap * h->NW);
+        if (!r) r = dalloc(h, &nc[s], newcap);
+        if (r) { drop(); return r; }
     }
-    h->bytes = saved - (h->cap > 0 ? 2 * h->cap * (2 * h->NW * 8 + 8) : 0);
-    h->z[0] = nz; h->x[0] = nx; h->c[0] = nc;
-    TRY(dalloc(h, &h->z[1], newcap * h->NW));
-    TRY(dalloc(h, &h->x[1], newcap * h->NW));
-    TRY(dalloc(h, &h->c[1], newcap));
+    cudaError_t ce = cudaSuccess;
+    if (have && st.n > 0) {
+        ce = cudaMemcpyAsync(nz[0], h->z[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(nx[0], h->x[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(nc[0], h->c[st.cur], st.n * 8, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) { drop(); return fail(PP_DEVICE_ERROR, cudaGetErrorString(ce)); }
+    for (int s = 0; s < 2; ++s) {
+        dfree(h, h->z[s]); dfree(h, h->x[s]); dfree(h, h->c[s]);
+        h->z[s] = nz[s]; h->x[s] = nx[s]; h->c[s] = nc[s];
+    }
+    if (have) {
+        // the live terms are in set 0 from here on, whatever fails below
+        st.cur = 0;
+        TRY(write_state(h, &st));
+    }
     TRY(dalloc(h, &h->srcidx, newcap + SEG));
     TRY(dalloc(h, &h->meta, newcap + SEG));
     TRY(dalloc(h, &h->src, newcap + SEG));
@@ -236,10 +274,6 @@ static int grow_live(pp_spv *h, long long need) {
     TRY(dalloc(h, &h->bwdA, ta * TAU_MAX));
     h->cap = newcap;
     TRY(alloc_merge_ws(h));
-    if (have) {
-        st.cur = 0;
-        TRY(write_state(h, &st));
-    }
     return PP_OK;
 }
 
@@ -254,16 +288,17 @@ static int ensure_append(pp_spv *h, long long need, long long pending) {
         long long nc = std::max(need, std::max(2 * h->acap_phys, (long long)4096));
         u64 *nz = nullptr, *nx = nullptr;
         double *ncc = nullptr;
-        TRY(dalloc(h, &nz, nc * h->NW));
-        TRY(dalloc(h, &nx, nc * h->NW));
-        TRY(dalloc(h, &ncc, nc));
+        int r = dalloc(h, &nz, nc * h->NW);
+        if (!r) r = dalloc(h, &nx, nc * h->NW);
+        if (!r) r = dalloc(h, &ncc, nc);
+        if (r) { dfree(h, nz); dfree(h, nx); dfree(h, ncc); return r; }
         if (pending > 0) {
             CU(cudaMemcpyAsync(nz, h->az, pending * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
             CU(cudaMemcpyAsync(nx, h->ax, pending * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
             CU(cudaMemcpyAsync(ncc, h->ac, pending * 8, cudaMemcpyDeviceToDevice, h->stream));
         }
         CU(cudaStreamSynchronize(h->stream));
-        if (h->az) { cudaFree(h->az); cudaFree(h->ax); cudaFree(h->ac); }
+        dfree(h, h->az); dfree(h, h->ax); dfree(h, h->ac);
         h->az = nz; h->ax = nx; h->ac = ncc;
         h->acap_phys = nc;
         TRY(alloc_merge_ws(h));
@@ -1352,10 +1387,13 @@ struct pp_mlp {
                         std::string(#call) + ": " + cudaGetErrorString(e_));                 \
     } while (0)
 
+// New buffer first, then the old one freed: a failure leaves *p as it was.
 template <typename T>
 static int malloc_n(T **p, long long n) {
-    if (*p) { cudaFree(*p); *p = nullptr; }
-    MCU(cudaMalloc((void **)p, (size_t)std::max(1ll, n) * sizeof(T)));
+    T *q = nullptr;
+    MCU(cudaMalloc((void **)&q, (size_t)std::max(1ll, n) * sizeof(T)));
+    if (*p) cudaFree(*p);
+    *p = q;
     return PP_OK;
 }
 
@@ -1562,13 +1600,19 @@ extern "C" int pp_features(pp_spv *h, const pp_feature_ctx *ctx, float *out, int
 }
 
 extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *ctx, int64_t budget,
-                                   float *cut_score) {
+                                   float *cut_score, pp_drop_sample *sample) {
     if (!h || !m || !ctx || budget < 0) return fail(PP_ARGUMENT_ERROR, "bad argument");
     if (h->NW != 1) return fail(PP_ARGUMENT_ERROR, "learned truncation needs N <= 64");
     DevState st;
     TRY(read_state(h, &st));
     if (cut_score) *cut_score = -INFINITY;
     const long long n = st.n;
+    if (sample) {
+        sample->n = 0;
+        sample->n_dropped = std::max(0ll, n - (long long)budget);
+        if (sample->cap < 0 || (sample->cap > 0 && (!sample->z || !sample->x || !sample->c)))
+            return fail(PP_ARGUMENT_ERROR, "bad drop-sample buffers");
+    }
     if (n <= budget) return PP_OK;
     MCU(cudaStreamSynchronize(m->stream));   // the network's last update is visible to h's stream
     if (n > m->score_cap) {
@@ -1603,12 +1647,37 @@ extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *c
     k_sel_scan<<<1, 1024, 0, s>>>(ntiles, m->sel, m->cgt, m->ceq, m->tie_off, m->out_off, m->total);
     k_sel_write<<<g, SL_THREADS, 0, s>>>(m->score, n, m->sel, m->tie_off, m->out_off, h->z[cur], h->x[cur], h->c[cur],
                                          h->z[cur ^ 1], h->x[cur ^ 1], h->c[cur ^ 1]);
+    u64 *sbuf = nullptr;
+    unsigned long long *scnt = nullptr;
+    long long scap = sample ? sample->cap : 0;
+    if (scap > 0) {
+        // acceptance probability 0.9 cap / dropped keeps the sample under its cap
+        const double pacc = std::min(1.0, 0.9 * (double)scap / (double)(n - budget));
+        const unsigned long long thr =
+            pacc >= 1.0 ? ~0ull : (unsigned long long)(pacc * 18446744073709551616.0);
+        CU(cudaMalloc((void **)&sbuf, (size_t)scap * 24 + 8));
+        scnt = reinterpret_cast<unsigned long long *>(sbuf + 3 * scap);
+        CU(cudaMemsetAsync(scnt, 0, 8, s));
+        k_sel_sample<<<h->nsm * 4, 256, 0, s>>>(m->score, n, m->sel, sample->seed, thr, h->z[cur], h->x[cur],
+                                               h->c[cur], sbuf, sbuf + scap, reinterpret_cast<double *>(sbuf + 2 * scap),
+                                               scap, scnt);
+    }
     CU(cudaGetLastError());
     long long kept = 0;
     SelectState sf;
     CU(cudaMemcpyAsync(&kept, m->total, sizeof kept, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&sf, m->sel, sizeof sf, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
+    if (scap > 0) {
+        unsigned long long got = 0;
+        cudaMemcpy(&got, scnt, 8, cudaMemcpyDeviceToHost);
+        const long long ns = std::min<long long>((long long)got, scap);
+        cudaMemcpy(sample->z, sbuf, ns * 8, cudaMemcpyDefault);
+        cudaMemcpy(sample->x, sbuf + scap, ns * 8, cudaMemcpyDefault);
+        cudaMemcpy(sample->c, sbuf + 2 * scap, ns * 8, cudaMemcpyDefault);
+        cudaFree(sbuf);
+        sample->n = ns;
+    }
     int e = 0;
     CU(cudaMemcpy(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
@@ -1627,5 +1696,52 @@ extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *c
         memcpy(&f, &u, 4);
         *cut_score = f;
     }
+    return PP_OK;
+}
+
+extern "C" int pp_sample_terms(pp_spv *h, int32_t nbins, double lg_lo, double lg_hi, int64_t per_bin, uint64_t seed,
+                               void *z, void *x, double *c, int64_t cap, int64_t *n_out) {
+    if (!h || !n_out || nbins < 1 || nbins > 64 || !(lg_hi > lg_lo) || per_bin < 0 || cap < 0 ||
+        (cap > 0 && (!z || !x || !c)))
+        return fail(PP_ARGUMENT_ERROR, "bad argument");
+    if (h->NW != 1) return fail(PP_ARGUMENT_ERROR, "term sampling needs N <= 64");
+    DevState st;
+    TRY(read_state(h, &st));
+    *n_out = 0;
+    const long long n = st.n;
+    if (n == 0 || cap == 0) return PP_OK;
+    cudaStream_t s = h->stream;
+    const int cur = st.cur;
+    unsigned long long *dbuf = nullptr;
+    CU(cudaMalloc((void **)&dbuf, (size_t)(2 * 64 + 1 + 3 * cap) * 8));
+    unsigned long long *hist = dbuf, *thr = dbuf + 64, *cnt = dbuf + 128;
+    u64 *sz = dbuf + 129, *sx = sz + cap;
+    double *sc = reinterpret_cast<double *>(sx + cap);
+    cudaMemsetAsync(dbuf, 0, 129 * 8, s);
+    k_lgc_hist<<<h->nsm * 4, 256, 0, s>>>(h->c[cur], n, lg_lo, lg_hi, nbins, hist);
+    unsigned long long hh[64], th[64];
+    cudaMemcpyAsync(hh, hist, nbins * 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { cudaFree(dbuf); return fail(PP_DEVICE_ERROR, cudaGetErrorString(e)); }
+    // acceptance 0.9 per_bin / count keeps the sample under its cap with high probability
+    for (int b = 0; b < nbins; ++b) {
+        const double p = hh[b] ? std::min(1.0, 0.9 * (double)per_bin / (double)hh[b]) : 0.0;
+        th[b] = p >= 1.0 ? ~0ull : (unsigned long long)(p * 18446744073709551616.0);
+    }
+    cudaMemcpyAsync(thr, th, nbins * 8, cudaMemcpyHostToDevice, s);
+    k_lgc_sample<<<h->nsm * 4, 256, 0, s>>>(h->z[cur], h->x[cur], h->c[cur], n, lg_lo, lg_hi, nbins, thr, seed, sz,
+                                             sx, sc, cap, cnt);
+    unsigned long long got = 0;
+    cudaMemcpyAsync(&got, cnt, 8, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    const long long ns = std::min<long long>((long long)got, cap);
+    if (e == cudaSuccess && ns > 0) {
+        cudaMemcpy(z, sz, ns * 8, cudaMemcpyDefault);
+        cudaMemcpy(x, sx, ns * 8, cudaMemcpyDefault);
+        e = cudaMemcpy(c, sc, ns * 8, cudaMemcpyDefault);
+    }
+    cudaFree(dbuf);
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, cudaGetErrorString(e));
+    *n_out = ns;
     return PP_OK;
 }

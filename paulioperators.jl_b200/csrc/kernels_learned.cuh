@@ -777,4 +777,66 @@ __global__ void k_sel_write(const float *score, long long n, const SelectState *
     }
 }
 
+// Uniform sample of the terms a cut drops (score key below the cut): term i is
+// taken when a hash of (seed, i) falls below thr, i.e. with probability thr / 2^64;
+// at most cap of them are written (their order is that of arrival).
+__global__ void k_sel_sample(const float *score, long long n, const SelectState *sel, unsigned long long seed,
+                             unsigned long long thr, const u64 *Z, const u64 *X, const double *C, u64 *sz, u64 *sx,
+                             double *sc, long long cap, unsigned long long *cnt) {
+    const unsigned cut = sel->prefix;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (fkey(score[i]) >= cut) continue;
+        unsigned long long h = seed ^ ((unsigned long long)i * 0x9E3779B97F4A7C15ull);
+        h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+        h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+        h ^= h >> 31;
+        if (h >= thr) continue;
+        const unsigned long long pos = atomicAdd(cnt, 1ull);
+        if (pos < (unsigned long long)cap) {
+            sz[pos] = Z[i];
+            sx[pos] = X[i];
+            sc[pos] = C[i];
+        }
+    }
+}
+
+// Stratified sampling of live terms by log10 |c|: nb bins of equal width over
+// [lo, hi) (values outside fall into the end bins).
+__device__ __forceinline__ int lgc_bin(double c, double lo, double hi, int nb) {
+    const double a = fabs(c);
+    const double l = a > 0.0 ? log10(a) : -300.0;
+    int b = (int)floor((l - lo) / (hi - lo) * nb);
+    return min(max(b, 0), nb - 1);
+}
+
+__global__ void k_lgc_hist(const double *C, long long n, double lo, double hi, int nb, unsigned long long *hist) {
+    __shared__ unsigned long long h[64];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        atomicAdd(&h[lgc_bin(C[i], lo, hi, nb)], 1ull);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// Term i of bin b is taken when a hash of (seed, i) falls below thr[b].
+__global__ void k_lgc_sample(const u64 *Z, const u64 *X, const double *C, long long n, double lo, double hi, int nb,
+                             const unsigned long long *thr, unsigned long long seed, u64 *sz, u64 *sx, double *sc,
+                             long long cap, unsigned long long *cnt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long h = seed ^ ((unsigned long long)i * 0x9E3779B97F4A7C15ull);
+        h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+        h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+        h ^= h >> 31;
+        if (h >= thr[lgc_bin(C[i], lo, hi, nb)]) continue;
+        const unsigned long long pos = atomicAdd(cnt, 1ull);
+        if (pos < (unsigned long long)cap) {
+            sz[pos] = Z[i];
+            sx[pos] = X[i];
+            sc[pos] = C[i];
+        }
+    }
+}
+
 }  // namespace pp

@@ -81,6 +81,11 @@ class PPFeatureCtx(Structure):
                 ("layer_frac", c_float), ("remaining_frac", c_float), ("theta_j", c_float), ("theta_h", c_float)]
 
 
+class PPDropSample(Structure):
+    _fields_ = [("cap", c_int64), ("seed", c_uint64), ("z", c_void_p), ("x", c_void_p), ("c", c_void_p),
+                ("n", c_int64), ("n_dropped", c_int64)]
+
+
 PP_MLP_NPARAM = 5313
 PP_STATS_LEN = 16
 STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
@@ -118,7 +123,10 @@ SIGNATURES = {
     "pp_mlp_load_data": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64]),
     "pp_mlp_train": (c_int32, [c_void_p, c_int64, c_int64, c_float, c_uint64, c_void_p]),
     "pp_features": (c_int32, [c_void_p, POINTER(PPFeatureCtx), c_void_p, c_int64, POINTER(c_int64)]),
-    "pp_learned_truncate": (c_int32, [c_void_p, c_void_p, POINTER(PPFeatureCtx), c_int64, POINTER(c_float)]),
+    "pp_learned_truncate": (c_int32, [c_void_p, c_void_p, POINTER(PPFeatureCtx), c_int64, POINTER(c_float),
+                                      POINTER(PPDropSample)]),
+    "pp_sample_terms": (c_int32, [c_void_p, c_int32, c_double, c_double, c_int64, c_uint64, c_void_p, c_void_p,
+                                  c_void_p, c_int64, POINTER(c_int64)]),
     "pp_last_error": (c_char_p, []),
 }
 
