@@ -431,12 +431,13 @@ def run_reference_batch(args, ctx, q, nthreads):
 
 LEARN = {
     "full": dict(n_train=8, n_test=3, sample_layers=(6, 10, 14), per_layer=6000, train_steps=4000, batch=8192,
-                 budgets=(1e6, 2e6, 5e6, 1e7, 2e7, 4e7), plain=(1e-5, 6e-6, 4e-6, 3e-6, 2e-6, 1.5e-6)),
+                 budgets=(5e6, 1e7, 2e7, 5e7, 1e8), plain=(1e-5, 3e-6, 2e-6, 1.5e-6, 1.2e-6, 1.1e-6)),
     "small": dict(n_train=2, n_test=1, sample_layers=(8, 12), per_layer=2000, train_steps=800, batch=4096,
                   budgets=(2e6, 1e7), plain=(1e-5, 3e-6)),
 }
-LEARN_T_REF, LEARN_T_BASE, LEARN_LABEL_T, LEARN_TOL = 1e-6, 1e-6, 1e-7, 1e-3
-LEARN_AUDIT = dict(layers=(5, 11), sample=1024, bound=2.5e-4, label_thresh=1e-7)
+# label threshold: 1e-3 x |c| (rounded up to a decade) per sampled term, floor 1e-12
+LEARN_T_REF, LEARN_T_BASE, LEARN_LABEL_T, LEARN_TOL = 1e-6, 1e-6, 1e-12, 1e-3
+LEARN_AUDIT = dict(layers=(5, 11), sample=1024, bound=2.5e-4, label_thresh=1e-12)
 
 
 def run_learned_bench(args):

@@ -98,6 +98,7 @@ struct pp_spv {
     int ncol = 0;
     bool batch_on = false;
     int *hfin = nullptr;
+    Select64 *sel64 = nullptr;                // AdaptiveTruncation's |c| select
     double *hpart = nullptr, *heout = nullptr;
     long long *hrange = nullptr, *hnout = nullptr;
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
@@ -599,7 +600,7 @@ extern "C" int pp_destroy(pp_spv *h) {
                     h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
                     h->S, h->P, h->gens, h->rec, h->sphys, h->soff, h->kcnt, h->split_k,
-                    h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout};
+                    h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout, h->sel64};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
@@ -842,13 +843,88 @@ static int general_boundary(pp_spv *h, int flags, long long *n_in, long long *n_
     return PP_OK;
 }
 
+// <ket|O|ket> of the live set (the reduction of pp_expect_ket).
+static int expect_dev(pp_spv *h, const u64 *k, double *out) {
+    Bufs B = make_bufs(h);
+    const int nb = std::min(4096, h->nsm * 8);
+    if (h->NW == 1) k_expect<1><<<nb, 256, 0, h->stream>>>(B, k[0], k[1], h->epart);
+    else k_expect<2><<<nb, 256, 0, h->stream>>>(B, k[0], k[1], h->epart);
+    k_expect_final<<<1, 32, 0, h->stream>>>(h->epart, nb, h->eout);
+    CU(cudaMemcpyAsync(out, h->eout, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return sync_check(h);
+}
+
+// _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114): with n > max_terms the
+// clip threshold is the (max_terms + 1)-th largest |c| -- coeffs[end - max_terms]
+// of the ascending sort -- found exactly by a radix select on the device;
+// otherwise min_thresh.  Then coeff_clip! (drop |c| <= thresh, order kept).
+static int adaptive_apply(pp_spv *h, long long max_terms, double min_thresh) {
+    DevState st;
+    TRY(read_state(h, &st));
+    double thr = min_thresh;
+    if (st.n > max_terms) {
+        if (!h->sel64) TRY(dalloc(h, &h->sel64, 1));
+        Select64 s0;
+        memset(&s0, 0, sizeof s0);
+        s0.remaining = max_terms + 1;
+        CU(cudaMemcpyAsync(h->sel64, &s0, sizeof s0, cudaMemcpyHostToDevice, h->stream));
+        const double *C = h->c[st.cur];
+        for (int shift = 56; shift >= 0; shift -= 8) {
+            k_abs_hist<<<h->nsm * 4, 256, 0, h->stream>>>(C, st.n, h->sel64, shift);
+            k_sel64_pick<<<1, 32, 0, h->stream>>>(h->sel64, shift);
+        }
+        Select64 sf;
+        CU(cudaMemcpyAsync(&sf, h->sel64, sizeof sf, cudaMemcpyDeviceToHost, h->stream));
+        TRY(sync_check(h));
+        memcpy(&thr, &sf.prefix, sizeof thr);
+    }
+    pp_filter f = NOFILTER_H;
+    f.thresh = thr;
+    compile_filter(&f, &h->Ph->clip);
+    TRY(upload_params(h));
+    TRY(read_state(h, &st));
+    st.an = 0;
+    TRY(write_state(h, &st));
+    Bufs B = make_bufs(h);
+    if (h->NW == 1) launch_merge<1, 2>(h, B, 0);
+    else launch_merge<2, 2>(h, B, 0);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    return check_err(h, st);
+}
+
+// AdaptiveTruncation as the evolve! truncation: applied after every (NOFILTER)
+// merge; with EnergyCorrection the energy change it causes is accumulated
+// (_boundary!, spv_evolve.jl:258-284).
+struct AdaptSpec {
+    bool on = false;
+    long long max_terms = 0;
+    double min_thresh = 0.0;
+    bool corr = false;
+    u64 ket[2] = {0, 0};
+};
+
+static int adapt_step(pp_spv *h, const AdaptSpec &A) {
+    double before = 0.0, after = 0.0;
+    if (A.corr) TRY(expect_dev(h, A.ket, &before));
+    TRY(adaptive_apply(h, A.max_terms, A.min_thresh));
+    if (A.corr) {
+        TRY(expect_dev(h, A.ket, &after));
+        DevState st;
+        TRY(read_state(h, &st));
+        st.corr_energy += after - before;
+        TRY(write_state(h, &st));
+    }
+    return PP_OK;
+}
+
 // General path: the sequence driver of spv_evolve.jl:352-385 with host decisions.
 // `period` > 0 makes every period-th rotation end a separate evolve! call (the
 // window count restarts and a boundary closes the layer), which is the
 // semantics of a loop "evolve!(v, layer; ...); channel!(v, p)".
 template <int NW>
 static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window, pp_counters *ctr, int last_flags,
-                       long long period, int chan_flags, RunProf *prof) {
+                       long long period, int chan_flags, RunProf *prof, const AdaptSpec &A) {
     const long long L = (long long)G.size();
     long long since = 0;
     for (long long i = 1; i <= L; ++i) {
@@ -859,6 +935,7 @@ static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window
         if (2 * st.an + st.n > st.acap_logical) {
             long long ni, no;
             TRY(general_boundary<NW>(h, 0, &ni, &no));
+            if (A.on) TRY(adapt_step(h, A));
             since = 0;
             TRY(read_state(h, &st));
             if (ctr && w <= ctr->nwin) {
@@ -897,7 +974,28 @@ static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window
             cudaEvent_t m0 = nullptr, m1 = nullptr;
             if (ctr && ctr->t_merge) { cudaEventCreate(&m0); cudaEventCreate(&m1); cudaEventRecord(m0, h->stream); }
             const int fl = (i == L ? last_flags : 0) | (layer_end ? chan_flags : 0);
-            TRY(general_boundary<NW>(h, fl, &ni, &no));
+            if (!A.on) {
+                TRY(general_boundary<NW>(h, fl, &ni, &no));
+            } else {
+                // merge unfiltered, then the strategy, then the layer's channel, then <ket|O|ket>
+                TRY(general_boundary<NW>(h, 0, &ni, &no));
+                TRY(adapt_step(h, A));
+                if (fl & GEN_CHANNEL) {
+                    Bufs Bc = make_bufs(h);
+                    k_channel<NW><<<h->nsm * 8, 256, 0, h->stream>>>(Bc);
+                    TRY(sync_check(h));
+                }
+                if (fl & GEN_MEASURE) {
+                    double e = 0.0;
+                    const u64 *kk = h->Ph->ket;
+                    TRY(expect_dev(h, kk, &e));
+                    DevState s2;
+                    TRY(read_state(h, &s2));
+                    s2.expect_val = e;
+                    s2.measure_valid = 1;
+                    TRY(write_state(h, &s2));
+                }
+            }
             prof->launches += 3;
             if (m0) {
                 cudaEventRecord(m1, h->stream);
@@ -927,7 +1025,16 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     if (O.window < 1) return fail(PP_ARGUMENT_ERROR, "window must be >= 1");
     if (L < 0) return fail(PP_DIMENSION_MISMATCH, "generators and angles must have same length");
     if (L > 0 && (!gz || !gx || !cosv || !sinv)) return fail(PP_ARGUMENT_ERROR, "null generator arrays");
-    if (O.strict_kind != 0) return fail(PP_NOT_IMPLEMENTED, "AdaptiveTruncation has no GPU merge path yet (no CPU fallback)");
+    if (O.strict_kind != 0 && O.strict_kind != 1) return fail(PP_ARGUMENT_ERROR, "unknown strict_kind");
+    AdaptSpec A;
+    if (O.strict_kind == 1) {
+        if (O.adapt_max_terms < 0) return fail(PP_ARGUMENT_ERROR, "max_terms must be >= 0");
+        A.on = true;
+        A.max_terms = O.adapt_max_terms;
+        A.min_thresh = O.adapt_min_thresh;
+        A.corr = O.corr_kind == 1;
+        load_word(O.ket, h->NW, A.ket);
+    }
     if (O.corr_kind != 0 && O.corr_kind != 1)
         return fail(PP_NOT_IMPLEMENTED, "only NoCorrection and EnergyCorrection run on the GPU");
     // parameters
@@ -986,7 +1093,7 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     pp_counters *ctr = O.counters;
     RunProf prof;
     prof.on = O.profile != 0;
-    if (O.window == 1 && all_struct) {
+    if (O.window == 1 && all_struct && !A.on) {
         TRY(ensure_live(h, 3 * st.n + 2 * SEG));
         const bool want_rec = ctr && ctr->nwin > 0;
         if (want_rec && L > h->rec_cap) {
@@ -1007,8 +1114,8 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
             }
         }
     } else {
-        if (h->NW == 1) TRY(run_general<1>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
-        else TRY(run_general<2>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof));
+        if (h->NW == 1) TRY(run_general<1>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof, A));
+        else TRY(run_general<2>(h, G, O.window, ctr, last_flags, period, GEN_CHANNEL, &prof, A));
     }
     TRY(read_state(h, &st));
     TRY(check_err(h, st));
@@ -1071,9 +1178,9 @@ extern "C" int pp_compact(pp_spv *h, const pp_filter *f) {
 }
 
 extern "C" int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh) {
-    (void)max_terms; (void)min_thresh;
     if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
-    return fail(PP_NOT_IMPLEMENTED, "AdaptiveTruncation has no GPU path yet (no CPU fallback)");
+    if (max_terms < 0) return fail(PP_ARGUMENT_ERROR, "max_terms must be >= 0");
+    return adaptive_apply(h, max_terms, min_thresh);
 }
 
 extern "C" int pp_channel(pp_spv *h, int32_t kind, const double *prm, const void *qubit_mask) {

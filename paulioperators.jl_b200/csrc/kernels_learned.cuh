@@ -839,4 +839,42 @@ __global__ void k_lgc_sample(const u64 *Z, const u64 *X, const double *C, long l
     }
 }
 
+// ------------------------------------------------------------------ |c| top-k select
+// Radix select over the 64-bit patterns of |c| (non-negative doubles order as
+// their bit patterns), 8 bits per pass from the top: the key of the
+// `remaining`-th largest |c|.  Used by AdaptiveTruncation.
+struct Select64 {
+    unsigned long long prefix, mask;
+    long long remaining;
+    unsigned hist[256];
+};
+
+__global__ void k_abs_hist(const double *C, long long n, Select64 *sel, int shift) {
+    __shared__ unsigned h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const unsigned long long pre = sel->prefix, msk = sel->mask;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = (unsigned long long)__double_as_longlong(fabs(C[i]));
+        if ((k & msk) == pre) atomicAdd(&h[(k >> shift) & 255ull], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&sel->hist[i], h[i]);
+}
+
+__global__ void k_sel64_pick(Select64 *sel, int shift) {
+    if (threadIdx.x != 0) return;
+    long long rem = sel->remaining;
+    int b = 255;
+    for (; b > 0; --b) {
+        if ((long long)sel->hist[b] >= rem) break;
+        rem -= sel->hist[b];
+    }
+    sel->prefix |= (unsigned long long)b << shift;
+    sel->mask |= 255ull << shift;
+    sel->remaining = rem;
+    for (int i = 0; i < 256; ++i) sel->hist[i] = 0;
+}
+
 }  // namespace pp

@@ -239,15 +239,12 @@ def run_plain(lat, draw, thresh):
 
 
 def coeff_truncate_(v, budget):
-    """The budget truncation without the network: keeps the `budget` terms of
-    largest |c| (ties: the smaller key), on the host."""
-    n = len(v)
-    if n <= budget:
-        return
-    z, x, c = v.to_arrays()
-    o = np.lexsort((np.arange(n), -np.abs(c)))[:budget]
-    o.sort()
-    v.upload(z[o], x[o], c[o], sorted=True)
+    """The budget truncation without the network: the reference's
+    AdaptiveTruncation(budget, 0) (keep the terms above the (budget+1)-th largest
+    |c|), on the device."""
+    from .spv import truncate_
+    from .truncation import AdaptiveTruncation
+    truncate_(v, AdaptiveTruncation(int(budget), 0.0))
 
 
 def run_learned(lat, draw, mlp, budget, t_base, audit=None):
@@ -332,10 +329,11 @@ def exact_contributions(lat, draw, z, x, c, layer, label_thresh, chunk=2048):
     return out
 
 
-def label_thresholds(c, base, rel=1e-5):
-    """Label threshold of each term: `base`, raised to rel x (the term's |c| rounded
-    up to a power of ten) for large terms, so that a term is labelled to relative
-    precision ~rel and the labelling work does not grow with |c| / base."""
+def label_thresholds(c, base, rel=1e-3):
+    """Label threshold of each term: rel x (the term's |c| rounded up to a power of
+    ten), never below `base`: every term is propagated to the same relative
+    precision, so small terms near the truncation cut keep their (collectively
+    large) contributions and large terms do not cost more than small ones."""
     a = np.maximum(np.abs(np.asarray(c, dtype=np.float64)), 1e-300)
     return np.maximum(base, rel * 10.0 ** np.ceil(np.log10(a)))
 
