@@ -474,6 +474,7 @@ static int launch_setup(pp_spv *h) {
     CU(cudaFuncSetAttribute(k_classify<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(2 * NW * A_TILE * 8 + A_TILE)));
     CU(cudaFuncSetAttribute(k_merge<NW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    CU(cudaFuncSetAttribute(k_tilescan<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tilescan_smem<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
     int occ = 0;
@@ -493,7 +494,7 @@ template <int NW>
 static void launch_struct_rotation(pp_spv *h, const Bufs &B) {
     cudaStream_t s = h->stream;
     k_classify<NW><<<h->nsm * h->occA1, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE, s>>>(B);
-    k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
+    k_tilescan<NW><<<1, S_THREADS, tilescan_smem<NW>(), s>>>(B);
     k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
     k_partition<NW, 0><<<h->nsm * 4, P_THREADS, 0, s>>>(B);
     k_merge<NW, 0><<<h->nsm * h->occB, B_THREADS, merge_smem_bytes<NW>(), s>>>(B, 0);
@@ -760,7 +761,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
                 for (int q = 0; q < 5; ++q) cudaEventCreate(&e[q]);
                 cudaEventRecord(e[0], s);
                 k_classify<NW><<<h->nsm * h->occA1, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE, s>>>(B);
-                k_tilescan<NW><<<1, S_THREADS, 0, s>>>(B);
+                k_tilescan<NW><<<1, S_THREADS, tilescan_smem<NW>(), s>>>(B);
                 k_permute<NW><<<h->nsm * h->occA3, A_THREADS, 0, s>>>(B);
                 cudaEventRecord(e[1], s);
                 k_partition<NW, 0><<<h->nsm * 4, P_THREADS, 0, s>>>(B);

@@ -285,6 +285,137 @@ __device__ __forceinline__ Key<NW> agg_key(const u64 *w4) {
 
 // ---------------------------------------------------------------- A2 tilescan
 constexpr int S_THREADS = 1024;
+// Rotations with at most TS_CAP tiles and TS_TAU thresholds (every rotation of a
+// one- or two-qubit generator up to ~5M live terms) stage the tile aggregates in
+// shared memory with one coalesced pass; the scans then read shared memory only.
+constexpr int TS_CAP = 2048;
+constexpr int TS_TAU = 8;
+
+template <int NW>
+constexpr size_t tilescan_smem() {
+    return (size_t)TS_CAP * (4 * NW * 8 + 3 * 4 + 2 * TS_TAU * 2);
+}
+
+template <int NW>
+__device__ __forceinline__ Key<NW> ts_key(const u64 *k) {
+    Key<NW> r;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) { r.z[w] = k[w]; r.x[w] = k[NW + w]; }
+    return r;
+}
+
+// The tile scan of k_tilescan below, from shared-memory copies of the aggregates.
+template <int NW>
+__device__ void tilescan_cached(const Bufs &B, const GenRec &g, int ntiles, long long n, long long *sml, int *smi,
+                                int *svec) {
+    DevState *S = B.S;
+    extern __shared__ u64 tsm[];
+    u64 *skey = tsm;                                                  // [TS_CAP][4 NW]: first (z, x), last (z, x)
+    int *scnt = reinterpret_cast<int *>(tsm + (size_t)TS_CAP * 4 * NW);
+    int *soffa = scnt + TS_CAP;
+    int *shf = soffa + TS_CAP;
+    short *sfp = reinterpret_cast<short *>(shf + TS_CAP);             // [TS_CAP][TS_TAU]
+    short *slp = sfp + TS_CAP * TS_TAU;
+    const int tid = threadIdx.x;
+    const int ntau = 2 * g.k;
+    for (int t = tid; t < ntiles; t += S_THREADS) {
+        const TileAggA &A = B.aggA[t];
+        const int c = A.count;
+        scnt[t] = c;
+        if (c > 0) {
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                skey[t * 4 * NW + w] = A.first[w];
+                skey[t * 4 * NW + NW + w] = A.first[2 + w];
+                skey[t * 4 * NW + 2 * NW + w] = A.last[w];
+                skey[t * 4 * NW + 3 * NW + w] = A.last[2 + w];
+            }
+        }
+        for (int tau = 0; tau < ntau; ++tau) {
+            sfp[t * TS_TAU + tau] = A.firstpos[tau];
+            slp[t * TS_TAU + tau] = A.lastpos[tau];
+        }
+    }
+    __syncthreads();
+    const int tpt = (ntiles + S_THREADS - 1) / S_THREADS;
+    const int t0 = min(tid * tpt, ntiles), t1 = min(t0 + tpt, ntiles);
+    long long loc = 0;
+    for (int t = t0; t < t1; ++t) loc += scnt[t];
+    long long total;
+    long long run = block_excl_scan<S_THREADS>(loc, 0ll, OpSum(), sml, &total);
+    for (int t = t0; t < t1; ++t) { soffa[t] = (int)run; B.offA[t] = (int)run; run += scnt[t]; }
+    const long long slots = max(1ll, (n + total + B_D - 1) / B_D);
+    if (slots * SEG > B.cap || n + total > B.cap) {
+        if (tid == 0) { S->err |= ERR_OVERFLOW; S->need = slots * SEG + SEG; }
+        return;
+    }
+    if (tid == 0) S->a = total;
+    int lastne = -1;
+    for (int t = t0; t < t1; ++t) if (scnt[t] > 0) lastne = t;
+    int tot_i;
+    int carry = block_excl_scan<S_THREADS>(lastne, -1, OpMax(), smi, &tot_i);
+    for (int t = t0; t < t1; ++t) {
+        int hf = -1;
+        if (scnt[t] > 0) {
+            hf = carry >= 0 ? hdiff<NW>(ts_key<NW>(skey + carry * 4 * NW + 2 * NW), ts_key<NW>(skey + t * 4 * NW))
+                            : H_INF;
+            carry = t;
+        }
+        shf[t] = hf;
+        B.hfirstA[t] = hf;
+    }
+    const int itotal = (int)total;
+    auto tileL = [&](int t, int tau, int thr) {
+        int L = shf[t] >= thr ? soffa[t] : -1;
+        const int lp = slp[t * TS_TAU + tau];
+        if (lp >= 0) L = max(L, soffa[t] + lp);
+        return L;
+    };
+    auto tileF = [&](int t, int tau, int thr) {
+        if (shf[t] >= thr) return soffa[t];
+        const int fp = sfp[t * TS_TAU + tau];
+        return fp != 0x7fff ? soffa[t] + fp : 0x7fffffff;
+    };
+    for (int g0 = 0; g0 < ntau; g0 += TAUV) {
+        const int na = min(TAUV, ntau - g0);
+        int lm[TAUV], fm[TAUV];
+#pragma unroll
+        for (int c = 0; c < TAUV; ++c) { lm[c] = -1; fm[c] = 0x7fffffff; }
+        for (int t = t0; t < t1; ++t) {
+            if (scnt[t] == 0) continue;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    const int thr = tau_value(g, g0 + c);
+                    lm[c] = max(lm[c], tileL(t, g0 + c, thr));
+                    fm[c] = min(fm[c], tileF(t, g0 + c, thr));
+                }
+            }
+        }
+        block_excl_scan_vec<S_THREADS, TAUV>(lm, -1, OpMax(), svec, na);
+        block_excl_suffix_vec<S_THREADS, TAUV>(fm, 0x7fffffff, OpMin(), svec, na);
+        for (int t = t0; t < t1; ++t) {
+            const bool ne = scnt[t] > 0;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    B.fwdA[(long long)t * TAU_MAX + g0 + c] = lm[c];
+                    if (ne) lm[c] = max(lm[c], tileL(t, g0 + c, tau_value(g, g0 + c)));
+                }
+            }
+        }
+        for (int t = t1 - 1; t >= t0; --t) {
+            const bool ne = scnt[t] > 0;
+#pragma unroll
+            for (int c = 0; c < TAUV; ++c) {
+                if (c < na) {
+                    B.bwdA[(long long)t * TAU_MAX + g0 + c] = min(fm[c], itotal);
+                    if (ne) fm[c] = min(fm[c], tileF(t, g0 + c, tau_value(g, g0 + c)));
+                }
+            }
+        }
+    }
+}
 
 template <int NW>
 __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
@@ -301,6 +432,10 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
     __syncthreads();
     const long long n = S->n;
     const int ntiles = (int)S->nseg;
+    if (ntiles <= TS_CAP && 2 * g.k <= TS_TAU) {
+        tilescan_cached<NW>(B, g, ntiles, n, sml, smi, svec);
+        return;
+    }
     const int tpt = (ntiles + S_THREADS - 1) / S_THREADS;
     const int t0 = min(tid * tpt, ntiles), t1 = min(t0 + tpt, ntiles);
     // tile offsets
@@ -394,6 +529,102 @@ __global__ void __launch_bounds__(S_THREADS) k_tilescan(Bufs B) {
 // max-scan and one vector backward min-scan of per-thread aggregates, then each
 // thread re-scans its A_ITEMS items in registers.
 
+// Tiles with at most PW_CAP emitting terms (most of them: a rotation emits from
+// a small fraction of the live terms) are permuted by one warp each, lane l
+// owning items l*PW_ITEMS .. +PW_ITEMS-1, with the scans done by shuffles (no
+// block barriers); larger tiles take the block path below.
+constexpr int PW_ITEMS = 8;
+constexpr int PW_CAP = 32 * PW_ITEMS;
+
+template <int NW>
+__device__ __forceinline__ void permute_warp_tile(const Bufs &B, const GenRec &g, int t, int cnt, long long atot,
+                                                  int lane) {
+    const int off = B.offA[t];
+    const long long base = B.sphys[t];
+    const int j0 = lane * PW_ITEMS;
+    const int ntau = 2 * g.k;
+    int h[PW_ITEMS];
+    unsigned cls[PW_ITEMS];
+    int delta[PW_ITEMS];
+#pragma unroll
+    for (int q = 0; q < PW_ITEMS; ++q) {
+        const int j = j0 + q;
+        const bool valid = j < cnt;
+        const unsigned m = valid ? B.meta[base + j] : 0u;
+        h[q] = valid ? (j == 0 ? B.hfirstA[t] : (int)(m & 0xffu)) : -1;
+        cls[q] = m >> 8;
+        delta[q] = 0;
+    }
+    for (int g0 = 0; g0 < ntau; g0 += TAUV) {
+        const int na = min(TAUV, ntau - g0);
+        int fw[TAUV], bw[TAUV];
+#pragma unroll
+        for (int c = 0; c < TAUV; ++c) {
+            fw[c] = -1;
+            bw[c] = 0x7fffffff;
+            if (c < na) {
+                const int thr = tau_value(g, g0 + c);
+#pragma unroll
+                for (int q = 0; q < PW_ITEMS; ++q)
+                    if (h[q] >= thr) { fw[c] = off + j0 + q; bw[c] = min(bw[c], off + j0 + q); }
+            }
+        }
+        // exclusive max-scan of fw over lower lanes, exclusive min-scan of bw over higher lanes,
+        // then the carries from the other tiles
+#pragma unroll
+        for (int c = 0; c < TAUV; ++c) {
+            if (c < na) {
+                int v = fw[c], u = bw[c];
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int o = __shfl_up_sync(0xffffffffu, v, d);
+                    if (lane >= d) v = max(v, o);
+                    const int p = __shfl_down_sync(0xffffffffu, u, d);
+                    if (lane + d < 32) u = min(u, p);
+                }
+                int ev = __shfl_up_sync(0xffffffffu, v, 1);
+                int eu = __shfl_down_sync(0xffffffffu, u, 1);
+                if (lane == 0) ev = -1;
+                if (lane == 31) eu = 0x7fffffff;
+                fw[c] = max(ev, B.fwdA[(long long)t * TAU_MAX + g0 + c]);
+                bw[c] = min(eu, B.bwdA[(long long)t * TAU_MAX + g0 + c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < TAUV; c += 2) {
+            if (c + 1 >= na) continue;
+            const int i = (g0 + c) >> 1;
+            const int thr_ge = tau_value(g, g0 + c), thr_gt = tau_value(g, g0 + c + 1);
+            int last_ge = fw[c], last_gt = fw[c + 1];
+            int nxt_ge[PW_ITEMS], nxt_gt[PW_ITEMS];
+            int run_ge = bw[c], run_gt = bw[c + 1];
+#pragma unroll
+            for (int q = PW_ITEMS - 1; q >= 0; --q) {
+                nxt_ge[q] = run_ge;
+                nxt_gt[q] = run_gt;
+                if (h[q] >= thr_ge) run_ge = off + j0 + q;
+                if (h[q] >= thr_gt) run_gt = off + j0 + q;
+            }
+#pragma unroll
+            for (int q = 0; q < PW_ITEMS; ++q) {
+                if (h[q] >= thr_ge) last_ge = off + j0 + q;
+                if (h[q] >= thr_gt) last_gt = off + j0 + q;
+                if ((cls[q] >> i) & 1u) delta[q] -= last_ge - last_gt;
+                else delta[q] += nxt_gt[q] - nxt_ge[q];
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < PW_ITEMS; ++q) {
+        const int j = j0 + q;
+        if (j < cnt) {
+            const long long pos = (long long)off + j + delta[q];
+            if (pos >= 0 && pos < atot) B.src[pos] = B.srcidx[base + j];
+            else atomicOr(&B.S->err, ERR_BOUNDS);
+        }
+    }
+}
+
 template <int NW>
 __global__ void __launch_bounds__(A_THREADS, 2) k_permute(Bufs B) {
     DevState *S = B.S;
@@ -410,9 +641,19 @@ __global__ void __launch_bounds__(A_THREADS, 2) k_permute(Bufs B) {
     const long long atot = S->a;
     const int ntiles = (int)S->nseg;
     const int ntau = 2 * g.k;
+    {
+        const int lane = tid & 31;
+        const long long w0 = (long long)blockIdx.x * (A_THREADS / 32) + (tid >> 5);
+        const long long nw = (long long)gridDim.x * (A_THREADS / 32);
+        for (long long t = w0; t < ntiles; t += nw) {
+            const int cnt = B.aggA[t].count;
+            if (cnt == 0 || cnt > PW_CAP) continue;
+            permute_warp_tile<NW>(B, g, (int)t, cnt, atot, lane);
+        }
+    }
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int cnt = B.aggA[t].count;
-        if (cnt == 0) continue;
+        if (cnt <= PW_CAP) continue;   // empty, or done by a warp above
         const int off = B.offA[t];
         const long long base = B.sphys[t];
         for (int j = tid; j < cnt; j += A_THREADS) { smeta[j] = B.meta[base + j]; ssrc[j] = B.srcidx[base + j]; }
