@@ -49,6 +49,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "paulioperators.jl_b200"))
 
 BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
+# DRAM traffic of k_merge<1,0> per algorithmic byte, from one ncu capture of the 176
+# merge launches of layer 11 of this workload (dram__bytes_read.sum +
+# dram__bytes_write.sum = 115.1 MB per launch against B(n + a + m) = 150.9 MB:
+# the gathered sin branches re-read live terms that are still in L2); the
+# summary and its command are in profiles/k_merge_lattice64_layer11.md
+MERGE_TRAFFIC_PER_ALG_BYTE = 115.09 / 150.88
 SNAP_LAYER = 10                      # CPU-baseline sample: layer 11 from the layer-10 state
 
 
@@ -670,7 +676,12 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "frac": (achieved / hbm) if achieved else None,
+                         "traffic": (MERGE_TRAFFIC_PER_ALG_BYTE * merge_bytes / max(1.0, len(gens))
+                                     if w.name == "lattice64" else None),
+                         "traffic_unit": "bytes per merge launch (ncu-measured ratio x this step's mean "
+                                         "algorithmic bytes per launch)",
+                         "alg_bytes_per_launch": merge_bytes / max(1.0, len(gens)),
                          "kernel": "k_merge<1,0> (merge + reduce-by-key + filter + channel + compaction)",
                          "peak_source": src,
                          "pipeline_frac": pipe_bytes / (sp["t_rotate"] + sp["t_merge"] + sp["t_partition"]) / 1e9 / hbm,
