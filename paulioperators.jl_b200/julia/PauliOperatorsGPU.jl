@@ -10,7 +10,8 @@ module PauliOperatorsGPU
 
 using PauliOperators
 using PauliOperators: MergeFilter, NOFILTER, _compile_filter, _is_compilable, _pack, _unpack, _word_type,
-                      CorrectionAccumulator, NoCorrection, EnergyCorrection, AdaptiveTruncation
+                      CorrectionAccumulator, NoCorrection, EnergyCorrection, AdaptiveTruncation,
+                      TruncationStrategy, CompositeTruncation
 
 const LIB = get(ENV, "PAULIPROP_LIB", joinpath(@__DIR__, "..", "lib", "libpauliprop.so"))
 
@@ -164,6 +165,29 @@ PauliOperators.weight_damped_clip!(v::CuSparsePauliVector, a::Real, t::Real) =
     _compact!(v, WeightDampedTruncation(Float64(a), Float64(t)))
 PauliOperators.x_weight_damped_clip!(v::CuSparsePauliVector, a::Real, t::Real) =
     _compact!(v, XWeightDampedTruncation(Float64(a), Float64(t)))
+
+# _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114): exact top-k clip on the device
+function _adaptive!(v::CuSparsePauliVector, s::AdaptiveTruncation)
+    check(ccall((:pp_adaptive, LIB), Cint, (Ptr{Cvoid}, Int64, Float64), v.h, s.max_terms, s.min_thresh))
+    return v
+end
+
+# truncate!(O, strategy, corr) (truncation.jl:330-337) for the strategies with a device path
+function PauliOperators.truncate!(v::CuSparsePauliVector{N}, s::TruncationStrategy,
+                                  corr::CorrectionAccumulator=NoCorrection()) where {N}
+    before = corr isa EnergyCorrection ? expectation_value(v, corr.ψ) : 0.0
+    if s isa AdaptiveTruncation
+        _adaptive!(v, s)
+    elseif s isa CompositeTruncation
+        foreach(x -> PauliOperators.truncate!(v, x), s.strategies)
+    elseif _is_compilable(s)
+        _compact!(v, s)
+    else
+        throw(ArgumentError("$(typeof(s)) has no GPU path (no CPU fallback)"))
+    end
+    corr isa EnergyCorrection && (corr.accumulated_energy += expectation_value(v, corr.ψ) - before)
+    return v
+end
 
 # channels (channels.jl:203-265)
 function _channel!(v::CuSparsePauliVector{N,W}, kind::Integer, prm, qubits) where {N,W}
