@@ -64,7 +64,8 @@ typedef struct {
     const pp_filter *strict;      /* truncation (compiled); NULL = NoTruncation */
     const pp_filter *local;       /* local_truncation; NULL = NoTruncation */
     int32_t strict_kind;          /* 0 compiled MergeFilter, 1 AdaptiveTruncation (PP_NOT_IMPLEMENTED) */
-    int32_t corr_kind;            /* 0 NoCorrection, 1 EnergyCorrection (truncation.jl:255-266) */
+    int32_t corr_kind;            /* 0 NoCorrection, 1 EnergyCorrection (truncation.jl:255-266),
+                                     2 EnergyVarianceCorrection (truncation.jl:269-278) */
     int64_t adapt_max_terms;
     double adapt_min_thresh;
     const void *ket;              /* EnergyCorrection ket: one word (type as z/x) */
@@ -81,6 +82,7 @@ typedef struct {
     double *stats_out;            /* nullable, PP_STATS_LEN doubles: see PP_STAT_* */
     int32_t profile;              /* 1: time the rotate and merge kernels with CUDA events (stats) */
     int32_t pad2;
+    double *corr_variance;        /* in/out: EnergyVarianceCorrection.accumulated_variance (corr_kind 2) */
 } pp_evolve_opts;
 
 /* stats_out layout (sums over the call's rotations). */
@@ -246,6 +248,8 @@ int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh);
  * pauli_channel! (203-221, 4).  prm: p, or pX,pY,pZ for kind 4.  qubit_mask: one
  * word (NULL = all qubits) as _spv_mask (channels.jl:200-201). */
 int pp_channel(pp_spv *h, int32_t kind, const double *prm, const void *qubit_mask);
+/* variance(v, ::Ket) (statistics.jl:6-22): <psi|O^2|psi> - <psi|O|psi>^2.  ket: one word. */
+int pp_variance(pp_spv *h, const void *ket, double *out);
 /* expectation_value(v, ::Ket) (spv_evolve.jl:133-134) -> _expectation_spv
  * (spv_kernels.jl:441-452).  ket: one word. */
 int pp_expect_ket(pp_spv *h, const void *ket, double *out);

@@ -99,6 +99,7 @@ struct pp_spv {
     bool batch_on = false;
     int *hfin = nullptr;
     Select64 *sel64 = nullptr;                // AdaptiveTruncation's |c| select
+    double *vtmp = nullptr;                   // variance: sigma[psi]
     double *hpart = nullptr, *heout = nullptr;
     long long *hrange = nullptr, *hnout = nullptr;
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
@@ -601,7 +602,7 @@ extern "C" int pp_destroy(pp_spv *h) {
                     h->offA, h->hfirstA, h->fwdA, h->bwdA, h->split_i, h->split_j, h->tstat, h->gstat, h->part,
                     h->az, h->ax, h->ac, h->tz, h->tx, h->tc, h->rhist, h->rsums, h->orand, h->epart, h->eout,
                     h->S, h->P, h->gens, h->rec, h->sphys, h->soff, h->kcnt, h->split_k,
-                    h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout, h->sel64};
+                    h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout, h->sel64, h->vtmp};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     if (h->Ph) cudaFreeHost(h->Ph);
@@ -894,27 +895,89 @@ static int adaptive_apply(pp_spv *h, long long max_terms, double min_thresh) {
     return check_err(h, st);
 }
 
-// AdaptiveTruncation as the evolve! truncation: applied after every (NOFILTER)
-// merge; with EnergyCorrection the energy change it causes is accumulated
-// (_boundary!, spv_evolve.jl:258-284).
+// variance(O, ψ) of the live set (statistics.jl:6-22; see k_var_records).
+template <int NW>
+static int variance_nw(pp_spv *h, const u64 *ket, double *out) {
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long n = st.n;
+    *out = 0.0;
+    if (n == 0) return PP_OK;
+    if (!h->vtmp) TRY(dalloc(h, &h->vtmp, 2));
+    TRY(ensure_append(h, std::max(n, h->acap_phys), 0));
+    Bufs B = make_bufs(h);
+    cudaStream_t s = h->stream;
+    k_var_records<NW><<<h->nsm * 8, 256, 0, s>>>(B, ket[0], ket[1], h->az, h->ax, h->ac);
+    int in_t = 0;
+    TRY(radix_sort<NW>(h, h->az, h->ax, h->ac, h->tz, h->tx, h->tc, n, &in_t));
+    const u64 *RZ = in_t ? h->tz : h->az, *RX = in_t ? h->tx : h->ax;
+    const double *RC = in_t ? h->tc : h->ac;
+    double *gval = in_t ? h->ac : h->tc;
+    CU(cudaMemsetAsync(h->vtmp, 0, 2 * sizeof(double), s));
+    k_var_groups<NW><<<h->nsm * 8, 256, 0, s>>>(RZ, RX, RC, n, gval, h->vtmp);
+    const int nb = std::min(4096, h->nsm * 8);
+    k_sum_partials<<<nb, 256, 0, s>>>(gval, n, h->epart);
+    k_expect_final<<<1, 32, 0, s>>>(h->epart, nb, h->eout);
+    double e2 = 0.0, e1 = 0.0;
+    CU(cudaMemcpyAsync(&e2, h->eout, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&e1, h->vtmp, sizeof(double), cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    *out = e2 - e1 * e1;
+    return PP_OK;
+}
+
+static int variance_dev(pp_spv *h, const u64 *ket, double *out) {
+    return h->NW == 1 ? variance_nw<1>(h, ket, out) : variance_nw<2>(h, ket, out);
+}
+
+// Truncations that run as a separate step after an unfiltered merge
+// (_boundary!, spv_evolve.jl:258-284): AdaptiveTruncation (_apply!), and any
+// truncation under EnergyVarianceCorrection (_needs_merged_measure: merge with
+// NOFILTER, measure, compact with the strict filter, measure).  The energy (and
+// variance) change the step causes is accumulated.
 struct AdaptSpec {
     bool on = false;
+    bool adaptive = false;            // AdaptiveTruncation, else the compiled strict filter
     long long max_terms = 0;
     double min_thresh = 0.0;
-    bool corr = false;
+    pp_filter strict = NOFILTER_H;
+    bool corr = false;                // EnergyCorrection or EnergyVarianceCorrection
+    bool var = false;                 // EnergyVarianceCorrection
     u64 ket[2] = {0, 0};
+    double var_acc = 0.0;             // accumulated variance change of this call
 };
 
-static int adapt_step(pp_spv *h, const AdaptSpec &A) {
-    double before = 0.0, after = 0.0;
+static int compact_with(pp_spv *h, const pp_filter &f) {
+    compile_filter(&f, &h->Ph->clip);
+    TRY(upload_params(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    st.an = 0;
+    TRY(write_state(h, &st));
+    Bufs B = make_bufs(h);
+    if (h->NW == 1) launch_merge<1, 2>(h, B, 0);
+    else launch_merge<2, 2>(h, B, 0);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    return check_err(h, st);
+}
+
+static int adapt_step(pp_spv *h, AdaptSpec &A) {
+    double before = 0.0, after = 0.0, vb = 0.0, va = 0.0;
     if (A.corr) TRY(expect_dev(h, A.ket, &before));
-    TRY(adaptive_apply(h, A.max_terms, A.min_thresh));
+    if (A.var) TRY(variance_dev(h, A.ket, &vb));
+    if (A.adaptive) TRY(adaptive_apply(h, A.max_terms, A.min_thresh));
+    else TRY(compact_with(h, A.strict));
     if (A.corr) {
         TRY(expect_dev(h, A.ket, &after));
         DevState st;
         TRY(read_state(h, &st));
         st.corr_energy += after - before;
         TRY(write_state(h, &st));
+    }
+    if (A.var) {
+        TRY(variance_dev(h, A.ket, &va));
+        A.var_acc += va - vb;
     }
     return PP_OK;
 }
@@ -925,7 +988,7 @@ static int adapt_step(pp_spv *h, const AdaptSpec &A) {
 // semantics of a loop "evolve!(v, layer; ...); channel!(v, p)".
 template <int NW>
 static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window, pp_counters *ctr, int last_flags,
-                       long long period, int chan_flags, RunProf *prof, const AdaptSpec &A) {
+                       long long period, int chan_flags, RunProf *prof, AdaptSpec &A) {
     const long long L = (long long)G.size();
     long long since = 0;
     for (long long i = 1; i <= L; ++i) {
@@ -1028,22 +1091,24 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     if (L > 0 && (!gz || !gx || !cosv || !sinv)) return fail(PP_ARGUMENT_ERROR, "null generator arrays");
     if (O.strict_kind != 0 && O.strict_kind != 1) return fail(PP_ARGUMENT_ERROR, "unknown strict_kind");
     AdaptSpec A;
-    if (O.strict_kind == 1) {
-        if (O.adapt_max_terms < 0) return fail(PP_ARGUMENT_ERROR, "max_terms must be >= 0");
+    if (O.strict_kind == 1 || O.corr_kind == 2) {
+        if (O.strict_kind == 1 && O.adapt_max_terms < 0) return fail(PP_ARGUMENT_ERROR, "max_terms must be >= 0");
         A.on = true;
+        A.adaptive = O.strict_kind == 1;
         A.max_terms = O.adapt_max_terms;
         A.min_thresh = O.adapt_min_thresh;
-        A.corr = O.corr_kind == 1;
+        if (O.strict_kind == 0 && O.strict) A.strict = *O.strict;
+        A.corr = O.corr_kind == 1 || O.corr_kind == 2;
+        A.var = O.corr_kind == 2;
         load_word(O.ket, h->NW, A.ket);
     }
-    if (O.corr_kind != 0 && O.corr_kind != 1)
-        return fail(PP_NOT_IMPLEMENTED, "only NoCorrection and EnergyCorrection run on the GPU");
-    // parameters
+    if (O.corr_kind < 0 || O.corr_kind > 2) return fail(PP_ARGUMENT_ERROR, "unknown corr_kind");
+    // parameters (a separate truncation step merges unfiltered and measures itself)
     DevParams *P = h->Ph;
-    compile_filter(O.strict, &P->strict);
+    compile_filter(A.on ? nullptr : O.strict, &P->strict);
     compile_filter(O.local, &P->local);
     P->local_active = filter_is_nofilter(O.local) ? 0 : 1;
-    P->corr_kind = O.corr_kind;
+    P->corr_kind = A.on ? 0 : O.corr_kind;
     load_word(O.ket, h->NW, P->ket);
     P->chan_kind = -1;
     if (O.chan_kind >= 0) TRY(build_channel(h, O.chan_kind, O.chan_prm, O.chan_mask, P));
@@ -1121,6 +1186,7 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     TRY(read_state(h, &st));
     TRY(check_err(h, st));
     if (O.corr_energy) *O.corr_energy = st.corr_energy;
+    if (O.corr_variance) *O.corr_variance += A.var_acc;
     if (O.expect_out) *O.expect_out = st.expect_val;
     if (O.stats_out) {
         double *so = O.stats_out;
@@ -1852,4 +1918,11 @@ extern "C" int pp_sample_terms(pp_spv *h, int32_t nbins, double lg_lo, double lg
     if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, cudaGetErrorString(e));
     *n_out = ns;
     return PP_OK;
+}
+
+extern "C" int pp_variance(pp_spv *h, const void *ket, double *out) {
+    if (!h || !out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    u64 k[2];
+    load_word(ket, h->NW, k);
+    return variance_dev(h, k, out);
 }

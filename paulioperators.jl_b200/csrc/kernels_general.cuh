@@ -306,6 +306,97 @@ __global__ void __launch_bounds__(256) k_expect(Bufs B, u64 k0, u64 k1, double *
     }
 }
 
+// ------------------------------------------------------------------ variance
+// variance(O, psi) (statistics.jl:6-22): sigma[x xor psi] += i^(thetas + 2 popc(z & (x xor psi))) c
+// over the live terms in storage order, thetas = (4 - popc(z & x) % 4) % 4
+// (symplectic_phase, type_PauliBasis.jl:36; PauliBasis * Ket, multiplication.jl:48-52);
+// Var = sum |sigma|^2 - sigma[psi]^2.  k_var_records writes one record per term:
+// key (x, flag) with flag 1 for an imaginary contribution, value +-c; a stable
+// sort by key then puts each sigma entry's real and imaginary contributions in
+// storage order, as the reference accumulates them.
+template <int NW>
+__global__ void k_var_records(Bufs B, u64 k0, u64 k1, u64 *RZ, u64 *RX, double *RC) {
+    DevState *S = B.S;
+    const long long n = S->n;
+    const int cur = S->cur;
+    const u64 *Z = B.z[cur], *X = B.x[cur];
+    const double *C = B.c[cur];
+    const u64 ket[2] = {k0, k1};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const Key<NW> k = load_key<NW>(Z, X, i);
+        int yc = 0, sg = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            yc += __popcll(k.z[w] & k.x[w]);
+            sg += __popcll(k.z[w] & (k.x[w] ^ ket[w]));
+        }
+        const int ph = ((4 - (yc & 3)) % 4 + 2 * (sg & 1)) & 3;   // power of i
+        Key<NW> r;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) { r.z[w] = k.x[w]; r.x[w] = 0; }
+        r.x[0] = (u64)(ph & 1);
+        store_key<NW>(RZ, RX, i, r);
+        RC[i] = ph >= 2 ? -C[i] : C[i];
+    }
+}
+
+// One thread per sigma entry (run of equal x in the sorted records): its real and
+// imaginary parts summed in record order; gval[i] = |sigma|^2 at the run's first
+// record (0 elsewhere), e1 = sigma[psi] (the x = 0 run, always real).
+template <int NW>
+__global__ void k_var_groups(const u64 *RZ, const u64 *RX, const double *RC, long long n, double *gval, double *e1) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const Key<NW> k = load_key<NW>(RZ, RX, i);
+        bool head = i == 0;
+        if (!head) {
+            const Key<NW> p = load_key<NW>(RZ, RX, i - 1);
+            bool same = true;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) same = same && p.z[w] == k.z[w];
+            head = !same;
+        }
+        if (!head) { gval[i] = 0.0; continue; }
+        double re = 0.0, im = 0.0;
+        for (long long j = i; j < n; ++j) {
+            const Key<NW> q = load_key<NW>(RZ, RX, j);
+            bool same = true;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) same = same && q.z[w] == k.z[w];
+            if (!same) break;
+            if (q.x[0] & 1ull) im = __dadd_rn(im, RC[j]);
+            else re = __dadd_rn(re, RC[j]);
+        }
+        gval[i] = __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
+        bool zero = true;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) zero = zero && k.z[w] == 0;
+        if (zero) *e1 = re;
+    }
+}
+
+// Compensated per-block partial sums of v[0, n) in block order (for k_expect_final).
+__global__ void __launch_bounds__(256) k_sum_partials(const double *v, long long n, double *partials) {
+    __shared__ double sm[256 / 32][2];
+    const long long per = (n + gridDim.x - 1) / gridDim.x;
+    const long long b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    Neu acc{0.0, 0.0};
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc.add(v[i]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double s = acc.s, c = acc.c;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, d);
+        c += __shfl_xor_sync(0xffffffffu, c, d);
+    }
+    if (lane == 0) { sm[warp][0] = s; sm[warp][1] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Neu t{0.0, 0.0};
+        for (int w = 0; w < 256 / 32; ++w) { t.add(sm[w][0]); t.add(sm[w][1]); }
+        partials[blockIdx.x] = t.s + t.c;
+    }
+}
+
 __global__ void k_expect_final(const double *partials, int nb, double *out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         Neu r{0.0, 0.0};

@@ -10,7 +10,8 @@ module PauliOperatorsGPU
 
 using PauliOperators
 using PauliOperators: MergeFilter, NOFILTER, _compile_filter, _is_compilable, _pack, _unpack, _word_type,
-                      CorrectionAccumulator, NoCorrection, EnergyCorrection, AdaptiveTruncation,
+                      CorrectionAccumulator, NoCorrection, EnergyCorrection, EnergyVarianceCorrection,
+                      AdaptiveTruncation,
                       TruncationStrategy, CompositeTruncation
 
 const LIB = get(ENV, "PAULIPROP_LIB", joinpath(@__DIR__, "..", "lib", "libpauliprop.so"))
@@ -48,6 +49,7 @@ struct PPEvolveOpts
     stats_out::Ptr{Float64}
     profile::Int32
     pad2::Int32
+    corr_variance::Ptr{Float64}
 end
 
 const ERRORS = Dict(1 => ArgumentError, 2 => DimensionMismatch)
@@ -133,22 +135,32 @@ function PauliOperators.evolve!(v::CuSparsePauliVector{N,W}, gens::Vector{PauliB
     loc = Ref(_compile_filter(local_truncation))
     kind = _is_compilable(truncation) ? Int32(0) : Int32(1)
     mt, mn = truncation isa AdaptiveTruncation ? (truncation.max_terms, truncation.min_thresh) : (0, 0.0)
-    ket = Ref{W}(zero(W)); ce = Ref(0.0); corr = Int32(0)
-    if correction isa EnergyCorrection
-        corr = Int32(1); ket[] = (correction.ψ.v % UInt128) % W; ce[] = correction.accumulated_energy
+    ket = Ref{W}(zero(W)); ce = Ref(0.0); cv = Ref(0.0); corr = Int32(0)
+    if correction isa Union{EnergyCorrection,EnergyVarianceCorrection}
+        corr = correction isa EnergyVarianceCorrection ? Int32(2) : Int32(1)
+        ket[] = (correction.ψ.v % UInt128) % W; ce[] = correction.accumulated_energy
+        correction isa EnergyVarianceCorrection && (cv[] = correction.accumulated_variance)
     end
-    GC.@preserve strict loc ket ce gz gx cs sn begin
+    GC.@preserve strict loc ket ce cv gz gx cs sn begin
         opts = Ref(PPEvolveOpts(window, Base.unsafe_convert(Ptr{MergeFilter}, strict),
                                 Base.unsafe_convert(Ptr{MergeFilter}, loc), kind, corr, mt, mn,
                                 Base.unsafe_convert(Ptr{W}, ket), Base.unsafe_convert(Ptr{Float64}, ce),
                                 C_NULL, Int32(-1), Int32(0), (0.0, 0.0, 0.0), C_NULL, C_NULL, 0, C_NULL,
-                                Int32(0), Int32(0)))
+                                Int32(0), Int32(0), Base.unsafe_convert(Ptr{Float64}, cv)))
         check(ccall((:pp_evolve, LIB), Cint,
                     (Ptr{Cvoid}, Ptr{W}, Ptr{W}, Ptr{Float64}, Ptr{Float64}, Int64, Ref{PPEvolveOpts}),
                     v.h, gz, gx, cs, sn, length(gens), opts))
     end
-    correction isa EnergyCorrection && (correction.accumulated_energy = ce[])
+    correction isa Union{EnergyCorrection,EnergyVarianceCorrection} && (correction.accumulated_energy = ce[])
+    correction isa EnergyVarianceCorrection && (correction.accumulated_variance = cv[])
     return v
+end
+
+# variance(v, ψ) (statistics.jl:6-22)
+function PauliOperators.variance(v::CuSparsePauliVector{N,W}, ψ::Ket{N}) where {N,W}
+    k = Ref((ψ.v % UInt128) % W); out = Ref(0.0)
+    check(ccall((:pp_variance, LIB), Cint, (Ptr{Cvoid}, Ref{W}, Ref{Float64}), v.h, k, out))
+    return out[]
 end
 
 # clip family (spv_evolve.jl:13-26) and compilable truncate! (truncation.jl:330-337)

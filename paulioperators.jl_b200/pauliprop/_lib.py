@@ -65,7 +65,7 @@ class PPEvolveOpts(Structure):
                 ("chan_prm", c_double * 3), ("chan_mask", c_void_p),
                 ("expect_out", POINTER(c_double)),
                 ("chan_every", c_int64), ("stats_out", POINTER(c_double)),
-                ("profile", c_int32), ("pad2", c_int32)]
+                ("profile", c_int32), ("pad2", c_int32), ("corr_variance", POINTER(c_double))]
 
 
 class PPBatch(Structure):
@@ -110,6 +110,7 @@ SIGNATURES = {
     "pp_adaptive": (c_int32, [c_void_p, c_int64, c_double]),
     "pp_channel": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
     "pp_expect_ket": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
+    "pp_variance": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
     "pp_check": (c_int32, [c_void_p, POINTER(c_int32)]),
     "pp_stream": (c_int32, [c_void_p, POINTER(c_void_p)]),
     "pp_device_bytes": (c_int32, [c_void_p, POINTER(c_int64)]),

@@ -24,8 +24,8 @@ from ._lib import (ArgumentError, DimensionMismatch, PPCounters, PPEvolveOpts, P
                    check, lib)
 from .paulis import PauliBasis, PauliSum, nwords, pack_keys, pack_word, qubit_mask, unpack_keys
 from .truncation import (NOFILTER, AdaptiveTruncation, CompositeTruncation, CorrectionAccumulator,
-                         EnergyCorrection, NoCorrection, NoTruncation, compile_filter,
-                         is_compilable)
+                         EnergyCorrection, EnergyVarianceCorrection, NoCorrection, NoTruncation,
+                         compile_filter, is_compilable)
 
 CHANNEL_KINDS = {"depolarizing": 0, "dephasing": 1, "bit_flip": 2, "bit_phase_flip": 3, "pauli": 4}
 
@@ -228,12 +228,16 @@ def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=Non
     opts.local = ctypes.pointer(local_f)
     ket = None
     ce = c_double(0.0)
-    if isinstance(correction, EnergyCorrection):
-        opts.corr_kind = 1
+    cv = c_double(0.0)
+    if isinstance(correction, (EnergyCorrection, EnergyVarianceCorrection)):
+        opts.corr_kind = 2 if isinstance(correction, EnergyVarianceCorrection) else 1
         ket = pack_word(v.N, correction.ket)
         opts.ket = _ptr(ket)
         ce.value = correction.accumulated_energy
         opts.corr_energy = ctypes.pointer(ce)
+        if isinstance(correction, EnergyVarianceCorrection):
+            cv.value = correction.accumulated_variance
+            opts.corr_variance = ctypes.pointer(cv)
     elif not isinstance(correction, NoCorrection):
         raise NotImplementedError(f"{type(correction).__name__} has no GPU path (no CPU fallback)")
     cc = counters._c() if counters is not None else None
@@ -260,8 +264,10 @@ def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=Non
     cosv = np.array([math.cos(a) for a in ang.tolist()], dtype=np.float64)
     sinv = np.array([math.sin(a) for a in ang.tolist()], dtype=np.float64)
     check(lib.pp_evolve(v._h, _ptr(gz), _ptr(gx), _ptr(cosv), _ptr(sinv), len(ang), byref(opts)))
-    if isinstance(correction, EnergyCorrection):
+    if isinstance(correction, (EnergyCorrection, EnergyVarianceCorrection)):
         correction.accumulated_energy = ce.value
+    if isinstance(correction, EnergyVarianceCorrection):
+        correction.accumulated_variance = cv.value
     if stats is not None:
         for name, i in _lib.STAT.items():
             stats[name] = float(st[i])
@@ -334,10 +340,14 @@ def _apply_(v, s):
 def truncate_(v, strategy, corr=None):
     """truncate!(O, strategy, corr) (truncation.jl:330-337)."""
     corr = corr or NoCorrection()
-    before = expectation_value(v, corr.ket) if isinstance(corr, EnergyCorrection) else None
+    track = isinstance(corr, (EnergyCorrection, EnergyVarianceCorrection))
+    before = expectation_value(v, corr.ket) if track else None
+    vbefore = variance(v, corr.ket) if isinstance(corr, EnergyVarianceCorrection) else None
     _apply_(v, strategy)
-    if isinstance(corr, EnergyCorrection):
+    if track:
         corr.accumulated_energy += expectation_value(v, corr.ket) - before
+        if vbefore is not None:
+            corr.accumulated_variance += variance(v, corr.ket) - vbefore
     elif not isinstance(corr, NoCorrection):
         raise NotImplementedError(f"{type(corr).__name__} has no GPU path (no CPU fallback)")
     return v
@@ -408,6 +418,15 @@ def expectation_value(v, ket):
     k = pack_word(v.N, int(ket))
     out = c_double()
     check(lib.pp_expect_ket(v._h, _ptr(k), byref(out)))
+    return out.value
+
+
+def variance(v, ket):
+    """variance(O, ψ) (statistics.jl:6-22): ⟨ψ|O²|ψ⟩ − ⟨ψ|O|ψ⟩² for a computational-basis
+    ket given as an integer bit mask."""
+    k = pack_word(v.N, int(ket))
+    out = c_double()
+    check(lib.pp_variance(v._h, _ptr(k), byref(out)))
     return out.value
 
 

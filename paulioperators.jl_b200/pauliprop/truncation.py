@@ -116,7 +116,7 @@ class EnergyCorrection(CorrectionAccumulator):
 
 
 class EnergyVarianceCorrection(CorrectionAccumulator):
-    """Energy and variance tracking (truncation.jl:273-278); no GPU path yet."""
+    """Energy and variance tracking (truncation.jl:269-278)."""
 
     def __init__(self, ket):
         self.ket = int(ket)

@@ -48,6 +48,28 @@ def test_power_table_matches_oracle_bitwise():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(_lib.PPFilter) == 64
-    assert ctypes.sizeof(_lib.PPEvolveOpts) == 144
-    assert ctypes.sizeof(_lib.PPCounters) == 56
+    """The ctypes mirrors have the sizes and field offsets of include/pauliprop.h's
+    structs, as gcc lays them out."""
+    import os
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    structs = {"pp_filter": _lib.PPFilter, "pp_evolve_opts": _lib.PPEvolveOpts, "pp_counters": _lib.PPCounters,
+               "pp_batch": _lib.PPBatch, "pp_feature_ctx": _lib.PPFeatureCtx, "pp_drop_sample": _lib.PPDropSample}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pauliprop.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "l.c"), os.path.join(d, "l")
+        with open(src, "w") as f:
+            f.write("\n".join(lines))
+        subprocess.run(["gcc", "-I", os.path.join(root, "include"), src, "-o", exe], check=True)
+        out = dict(l.rsplit(" ", 1) for l in subprocess.run([exe], check=True, capture_output=True,
+                                                            text=True).stdout.split("\n") if l)
+    for cname, py in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(out[f"{cname}.{fname}"]) == getattr(py, fname).offset, (cname, fname)
