@@ -63,7 +63,10 @@ typedef struct {
     int64_t window;               /* window = 1 (default) */
     const pp_filter *strict;      /* truncation (compiled); NULL = NoTruncation */
     const pp_filter *local;       /* local_truncation; NULL = NoTruncation */
-    int32_t strict_kind;          /* 0 compiled MergeFilter, 1 AdaptiveTruncation (PP_NOT_IMPLEMENTED) */
+    int32_t strict_kind;          /* 0 compiled MergeFilter, 1 AdaptiveTruncation (adapt_max_terms,
+                                     adapt_min_thresh), 2 StochasticCoeffTruncation (epsilon in
+                                     adapt_min_thresh), 3 StochasticSamplingTruncation (n_keep in
+                                     adapt_max_terms); 1-3 run after every unfiltered merge */
     int32_t corr_kind;            /* 0 NoCorrection, 1 EnergyCorrection (truncation.jl:255-266),
                                      2 EnergyVarianceCorrection (truncation.jl:269-278) */
     int64_t adapt_max_terms;
@@ -83,6 +86,7 @@ typedef struct {
     int32_t profile;              /* 1: time the rotate and merge kernels with CUDA events (stats) */
     int32_t pad2;
     double *corr_variance;        /* in/out: EnergyVarianceCorrection.accumulated_variance (corr_kind 2) */
+    uint64_t seed;                /* strict_kind 2, 3: random stream (application k uses its own substream) */
 } pp_evolve_opts;
 
 /* stats_out layout (sums over the call's rotations). */
@@ -243,6 +247,12 @@ int pp_compact_static(int32_t N, const void *z, const void *x, const double *c, 
                       void *z_out, void *x_out, double *c_out, int64_t *n_out, void *stream);
 /* _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114). */
 int pp_adaptive(pp_spv *h, int64_t max_terms, double min_thresh);
+/* stochastic_clip!(v, epsilon) (spv_evolve.jl:35-52) and _apply!(v,
+ * ::StochasticSamplingTruncation) (spv_evolve.jl:69-99).  Random numbers come from a
+ * counter-based generator keyed by seed and term index (the reference's Julia RNG
+ * stream cannot be reproduced; results agree in distribution). */
+int pp_stochastic_clip(pp_spv *h, double epsilon, uint64_t seed);
+int pp_stochastic_sample(pp_spv *h, int64_t n_keep, uint64_t seed);
 /* depolarizing_channel! (channels.jl:223-232, kind 0), dephasing_channel! (234-243, 1),
  * bit_flip_channel! (245-254, 2), bit_phase_flip_channel! (256-265, 3),
  * pauli_channel! (203-221, 4).  prm: p, or pX,pY,pZ for kind 4.  qubit_mask: one

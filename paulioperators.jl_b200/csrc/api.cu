@@ -23,6 +23,7 @@
 #include "kernels_general.cuh"
 #include "kernels_batch.cuh"
 #include "kernels_learned.cuh"
+#include "kernels_stoch.cuh"
 
 using namespace pp;
 
@@ -930,6 +931,114 @@ static int variance_dev(pp_spv *h, const u64 *ket, double *out) {
     return h->NW == 1 ? variance_nw<1>(h, ket, out) : variance_nw<2>(h, ket, out);
 }
 
+// Device scratch of one stochastic truncation call (freed on return).
+struct Scratch {
+    std::vector<void *> p;
+    ~Scratch() { for (void *q : p) cudaFree(q); }
+    template <typename T>
+    int get(T **out, long long count) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, (size_t)std::max(1ll, count) * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PP_OUT_OF_MEMORY, "cudaMalloc (stochastic truncation scratch)");
+        }
+        p.push_back(q);
+        *out = (T *)q;
+        return PP_OK;
+    }
+};
+
+// Commits an order-preserving flag compaction of the live set into the other set.
+static int flag_compact(pp_spv *h, DevState &st, const unsigned char *keep, const double *nc, const double *scale,
+                        Scratch &sc) {
+    const long long n = st.n;
+    const long long ntiles = (n + FC_TILE - 1) / FC_TILE;
+    int *cnt, *off;
+    long long *total;
+    TRY(sc.get(&cnt, ntiles));
+    TRY(sc.get(&off, ntiles));
+    TRY(sc.get(&total, 1));
+    cudaStream_t s = h->stream;
+    const int cur = st.cur;
+    const int g = (int)std::min<long long>(ntiles, 8ll * h->nsm);
+    k_flag_count<<<g, FC_THREADS, 0, s>>>(keep, n, cnt);
+    k_flag_scan<<<1, 1024, 0, s>>>(ntiles, cnt, off, total);
+    k_flag_write<<<g, FC_THREADS, 0, s>>>(keep, n, off, h->z[cur], h->x[cur], h->c[cur], nc, h->NW, scale,
+                                          h->z[cur ^ 1], h->x[cur ^ 1], h->c[cur ^ 1]);
+    long long kept = 0;
+    CU(cudaMemcpyAsync(&kept, total, sizeof kept, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    st.n = kept;
+    st.cur ^= 1;
+    return write_state(h, &st);
+}
+
+// stochastic_clip!(v, eps) (spv_evolve.jl:35-52) with the counter-based generator.
+static int stoch_clip_apply(pp_spv *h, double eps, unsigned long long seed) {
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long n = st.n;
+    if (n == 0) return PP_OK;
+    Scratch sc;
+    unsigned char *keep;
+    double *nc;
+    TRY(sc.get(&keep, n));
+    TRY(sc.get(&nc, n));
+    k_stoch_clip_mark<<<h->nsm * 8, 256, 0, h->stream>>>(h->c[st.cur], n, eps, seed, keep, nc);
+    return flag_compact(h, st, keep, nc, nullptr, sc);
+}
+
+// _apply!(v, ::StochasticSamplingTruncation) (spv_evolve.jl:69-99): the n_keep
+// largest keys u^(1/|c|^2) (exact radix select; ties: the smaller index), then
+// the norm-restoring scale.
+static int stoch_sample_apply(pp_spv *h, long long n_keep, unsigned long long seed) {
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long n = st.n;
+    if (n <= n_keep) return PP_OK;
+    Scratch sc;
+    unsigned long long *key;
+    unsigned char *keep, *keyeq;
+    int *tcnt, *toff;
+    long long *ttot;
+    Select64 *sel;
+    double *pall, *pkept, *nrm;
+    const long long ntiles = (n + FC_TILE - 1) / FC_TILE;
+    const int nb = std::min(4096, h->nsm * 8);
+    TRY(sc.get(&key, n));
+    TRY(sc.get(&keep, n));
+    TRY(sc.get(&keyeq, n));
+    TRY(sc.get(&tcnt, ntiles));
+    TRY(sc.get(&toff, ntiles));
+    TRY(sc.get(&ttot, 1));
+    TRY(sc.get(&sel, 1));
+    TRY(sc.get(&pall, nb));
+    TRY(sc.get(&pkept, nb));
+    TRY(sc.get(&nrm, 3));
+    cudaStream_t s = h->stream;
+    const double *C = h->c[st.cur];
+    k_stoch_sample_keys<<<h->nsm * 8, 256, 0, s>>>(C, n, seed, key);
+    Select64 s0;
+    memset(&s0, 0, sizeof s0);
+    s0.remaining = n_keep;
+    CU(cudaMemcpyAsync(sel, &s0, sizeof s0, cudaMemcpyHostToDevice, s));
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        k_key64_hist<<<h->nsm * 4, 256, 0, s>>>(key, n, sel, shift);
+        k_sel64_pick<<<1, 32, 0, s>>>(sel, shift);
+    }
+    k_stoch_sample_mark<<<h->nsm * 8, 256, 0, s>>>(key, n, sel, keep, keyeq);
+    const int g = (int)std::min<long long>(ntiles, 8ll * h->nsm);
+    k_flag_count<<<g, FC_THREADS, 0, s>>>(keyeq, n, tcnt);
+    k_flag_scan<<<1, 1024, 0, s>>>(ntiles, tcnt, toff, ttot);
+    k_stoch_sample_ties<<<g, FC_THREADS, 0, s>>>(n, sel, keyeq, toff, keep);
+    k_norm_partials<<<nb, 256, 0, s>>>(C, keep, n, pall, pkept);
+    k_expect_final<<<1, 32, 0, s>>>(pall, nb, nrm);
+    k_expect_final<<<1, 32, 0, s>>>(pkept, nb, nrm + 1);
+    k_norm_scale<<<1, 32, 0, s>>>(nrm, nrm + 1, nrm + 2);
+    return flag_compact(h, st, keep, nullptr, nrm + 2, sc);
+}
+
 // Truncations that run as a separate step after an unfiltered merge
 // (_boundary!, spv_evolve.jl:258-284): AdaptiveTruncation (_apply!), and any
 // truncation under EnergyVarianceCorrection (_needs_merged_measure: merge with
@@ -937,7 +1046,11 @@ static int variance_dev(pp_spv *h, const u64 *ket, double *out) {
 // variance) change the step causes is accumulated.
 struct AdaptSpec {
     bool on = false;
-    bool adaptive = false;            // AdaptiveTruncation, else the compiled strict filter
+    int kind = 0;                     // 0 compiled strict filter, 1 Adaptive, 2 StochasticCoeff, 3 StochasticSampling
+    bool adaptive = false;            // kind == 1
+    double epsilon = 0.0;             // kind 2
+    unsigned long long seed = 0;      // kinds 2, 3: each application draws from seed + its index
+    long long napp = 0;
     long long max_terms = 0;
     double min_thresh = 0.0;
     pp_filter strict = NOFILTER_H;
@@ -966,7 +1079,10 @@ static int adapt_step(pp_spv *h, AdaptSpec &A) {
     double before = 0.0, after = 0.0, vb = 0.0, va = 0.0;
     if (A.corr) TRY(expect_dev(h, A.ket, &before));
     if (A.var) TRY(variance_dev(h, A.ket, &vb));
-    if (A.adaptive) TRY(adaptive_apply(h, A.max_terms, A.min_thresh));
+    const unsigned long long sd = A.seed + 0xD1B54A32D192ED03ull * (unsigned long long)(A.napp++);
+    if (A.kind == 1) TRY(adaptive_apply(h, A.max_terms, A.min_thresh));
+    else if (A.kind == 2) TRY(stoch_clip_apply(h, A.epsilon, sd));
+    else if (A.kind == 3) TRY(stoch_sample_apply(h, A.max_terms, sd));
     else TRY(compact_with(h, A.strict));
     if (A.corr) {
         TRY(expect_dev(h, A.ket, &after));
@@ -1089,12 +1205,16 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
     if (O.window < 1) return fail(PP_ARGUMENT_ERROR, "window must be >= 1");
     if (L < 0) return fail(PP_DIMENSION_MISMATCH, "generators and angles must have same length");
     if (L > 0 && (!gz || !gx || !cosv || !sinv)) return fail(PP_ARGUMENT_ERROR, "null generator arrays");
-    if (O.strict_kind != 0 && O.strict_kind != 1) return fail(PP_ARGUMENT_ERROR, "unknown strict_kind");
+    if (O.strict_kind < 0 || O.strict_kind > 3) return fail(PP_ARGUMENT_ERROR, "unknown strict_kind");
     AdaptSpec A;
-    if (O.strict_kind == 1 || O.corr_kind == 2) {
-        if (O.strict_kind == 1 && O.adapt_max_terms < 0) return fail(PP_ARGUMENT_ERROR, "max_terms must be >= 0");
+    if (O.strict_kind != 0 || O.corr_kind == 2) {
+        if ((O.strict_kind == 1 || O.strict_kind == 3) && O.adapt_max_terms < 0)
+            return fail(PP_ARGUMENT_ERROR, "max_terms / n_keep must be >= 0");
         A.on = true;
+        A.kind = O.strict_kind;
         A.adaptive = O.strict_kind == 1;
+        A.epsilon = O.adapt_min_thresh;
+        A.seed = O.seed;
         A.max_terms = O.adapt_max_terms;
         A.min_thresh = O.adapt_min_thresh;
         if (O.strict_kind == 0 && O.strict) A.strict = *O.strict;
@@ -1925,4 +2045,15 @@ extern "C" int pp_variance(pp_spv *h, const void *ket, double *out) {
     u64 k[2];
     load_word(ket, h->NW, k);
     return variance_dev(h, k, out);
+}
+
+extern "C" int pp_stochastic_clip(pp_spv *h, double epsilon, uint64_t seed) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    return stoch_clip_apply(h, epsilon, seed);
+}
+
+extern "C" int pp_stochastic_sample(pp_spv *h, int64_t n_keep, uint64_t seed) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    if (n_keep < 0) return fail(PP_ARGUMENT_ERROR, "n_keep must be >= 0");
+    return stoch_sample_apply(h, n_keep, seed);
 }

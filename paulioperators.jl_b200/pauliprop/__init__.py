@@ -19,7 +19,8 @@ from .spv import (SparsePauliVector, WindowCounters, bit_flip_channel, bit_flip_
                   depolarizing_channel_, depolarizing_p_for_weight_decay, evolve, evolve_,
                   expectation_value, majorana_weight_clip_, pauli_channel, pauli_channel_,
                   phase_flip_channel_, power_table, truncate_, weight_clip_,
-                  weight_damped_clip_, variance, x_weight_clip_, x_weight_damped_clip_)
+                  weight_damped_clip_, stochastic_clip_, variance, x_weight_clip_,
+                  x_weight_damped_clip_)
 from .batch import BatchResult, evolve_batch, split_instances, tagged_terms
 from .learned import MLP, features, lattice_feature_ctx, learned_truncate_
 from . import circuits

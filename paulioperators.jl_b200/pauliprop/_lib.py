@@ -65,7 +65,8 @@ class PPEvolveOpts(Structure):
                 ("chan_prm", c_double * 3), ("chan_mask", c_void_p),
                 ("expect_out", POINTER(c_double)),
                 ("chan_every", c_int64), ("stats_out", POINTER(c_double)),
-                ("profile", c_int32), ("pad2", c_int32), ("corr_variance", POINTER(c_double))]
+                ("profile", c_int32), ("pad2", c_int32), ("corr_variance", POINTER(c_double)),
+                ("seed", c_uint64)]
 
 
 class PPBatch(Structure):
@@ -111,6 +112,8 @@ SIGNATURES = {
     "pp_channel": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
     "pp_expect_ket": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
     "pp_variance": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
+    "pp_stochastic_clip": (c_int32, [c_void_p, c_double, c_uint64]),
+    "pp_stochastic_sample": (c_int32, [c_void_p, c_int64, c_uint64]),
     "pp_check": (c_int32, [c_void_p, POINTER(c_int32)]),
     "pp_stream": (c_int32, [c_void_p, POINTER(c_void_p)]),
     "pp_device_bytes": (c_int32, [c_void_p, POINTER(c_int64)]),

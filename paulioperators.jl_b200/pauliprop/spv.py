@@ -25,7 +25,8 @@ from ._lib import (ArgumentError, DimensionMismatch, PPCounters, PPEvolveOpts, P
 from .paulis import PauliBasis, PauliSum, nwords, pack_keys, pack_word, qubit_mask, unpack_keys
 from .truncation import (NOFILTER, AdaptiveTruncation, CompositeTruncation, CorrectionAccumulator,
                          EnergyCorrection, EnergyVarianceCorrection, NoCorrection, NoTruncation,
-                         compile_filter, is_compilable)
+                         StochasticCoeffTruncation, StochasticSamplingTruncation, compile_filter,
+                         draw_seed, is_compilable)
 
 CHANNEL_KINDS = {"depolarizing": 0, "dephasing": 1, "bit_flip": 2, "bit_phase_flip": 3, "pauli": 4}
 
@@ -222,6 +223,14 @@ def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=Non
         opts.strict_kind = 1
         opts.adapt_max_terms = truncation.max_terms
         opts.adapt_min_thresh = truncation.min_thresh
+    elif isinstance(truncation, StochasticCoeffTruncation):
+        opts.strict_kind = 2
+        opts.adapt_min_thresh = truncation.epsilon
+        opts.seed = draw_seed(truncation.rng)
+    elif isinstance(truncation, StochasticSamplingTruncation):
+        opts.strict_kind = 3
+        opts.adapt_max_terms = truncation.n_keep
+        opts.seed = draw_seed(truncation.rng)
     else:
         raise NotImplementedError(f"{type(truncation).__name__} has no GPU path (no CPU fallback)")
     local_f = _pp_filter(compile_filter(local_truncation))
@@ -334,6 +343,12 @@ def _apply_(v, s):
     if isinstance(s, AdaptiveTruncation):
         check(lib.pp_adaptive(v._h, s.max_terms, s.min_thresh))
         return v
+    if isinstance(s, StochasticCoeffTruncation):
+        check(lib.pp_stochastic_clip(v._h, s.epsilon, draw_seed(s.rng)))
+        return v
+    if isinstance(s, StochasticSamplingTruncation):
+        check(lib.pp_stochastic_sample(v._h, s.n_keep, draw_seed(s.rng)))
+        return v
     raise NotImplementedError(f"{type(s).__name__} has no GPU path (no CPU fallback)")
 
 
@@ -419,6 +434,14 @@ def expectation_value(v, ket):
     out = c_double()
     check(lib.pp_expect_ket(v._h, _ptr(k), byref(out)))
     return out.value
+
+
+def stochastic_clip_(v, epsilon, rng=None):
+    """stochastic_clip!(v, ε; rng) (spv_evolve.jl:35-52): a term with |c| < ε survives
+    with probability |c|/ε, promoted to ε·sign(c); rng seeds the device generator."""
+    import random as _random
+    check(lib.pp_stochastic_clip(v._h, float(epsilon), draw_seed(rng if rng is not None else _random.Random())))
+    return v
 
 
 def variance(v, ket):

@@ -66,20 +66,31 @@ class XWeightDampedTruncation(TruncationStrategy):
         self.thresh = float(thresh)
 
 
+def draw_seed(rng):
+    """A 64-bit seed for the device generator from a random.Random, a numpy
+    Generator or an integer (each use of a strategy draws a fresh one, so repeated
+    truncations are independent, as with the reference's advancing RNG)."""
+    if isinstance(rng, int):
+        return rng & ((1 << 64) - 1)
+    if hasattr(rng, "getrandbits"):
+        return rng.getrandbits(64)
+    return int(rng.integers(0, 1 << 63)) << 1 | int(rng.integers(0, 2))
+
+
 class StochasticCoeffTruncation(TruncationStrategy):
-    """Russian roulette (truncation.jl:113-117); no GPU path yet."""
+    """Russian roulette (truncation.jl:105-117); device random numbers seeded from rng."""
 
     def __init__(self, epsilon, rng=None):
         self.epsilon = float(epsilon)
-        self.rng = rng or random.Random()
+        self.rng = rng if rng is not None else random.Random()
 
 
 class StochasticSamplingTruncation(TruncationStrategy):
-    """|c|^2 importance sampling (truncation.jl:125-129); no GPU path yet."""
+    """|c|^2 importance sampling (truncation.jl:119-129); device random numbers seeded from rng."""
 
     def __init__(self, n_keep, rng=None):
         self.n_keep = int(n_keep)
-        self.rng = rng or random.Random()
+        self.rng = rng if rng is not None else random.Random()
 
 
 class AdaptiveTruncation(TruncationStrategy):
