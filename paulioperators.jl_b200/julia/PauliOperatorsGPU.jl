@@ -9,9 +9,10 @@
 module PauliOperatorsGPU
 
 using PauliOperators
+using Random
 using PauliOperators: MergeFilter, NOFILTER, _compile_filter, _is_compilable, _pack, _unpack, _word_type,
                       CorrectionAccumulator, NoCorrection, EnergyCorrection, EnergyVarianceCorrection,
-                      AdaptiveTruncation,
+                      AdaptiveTruncation, StochasticCoeffTruncation, StochasticSamplingTruncation,
                       TruncationStrategy, CompositeTruncation
 
 const LIB = get(ENV, "PAULIPROP_LIB", joinpath(@__DIR__, "..", "lib", "libpauliprop.so"))
@@ -50,6 +51,7 @@ struct PPEvolveOpts
     profile::Int32
     pad2::Int32
     corr_variance::Ptr{Float64}
+    seed::UInt64
 end
 
 const ERRORS = Dict(1 => ArgumentError, 2 => DimensionMismatch)
@@ -133,8 +135,16 @@ function PauliOperators.evolve!(v::CuSparsePauliVector{N,W}, gens::Vector{PauliB
     cs = cos.(Float64.(angles)); sn = sin.(Float64.(angles))
     strict = Ref(_is_compilable(truncation) ? _compile_filter(truncation) : NOFILTER)
     loc = Ref(_compile_filter(local_truncation))
-    kind = _is_compilable(truncation) ? Int32(0) : Int32(1)
-    mt, mn = truncation isa AdaptiveTruncation ? (truncation.max_terms, truncation.min_thresh) : (0, 0.0)
+    kind, mt, mn, seed = Int32(0), 0, 0.0, UInt64(0)
+    if truncation isa AdaptiveTruncation
+        kind, mt, mn = Int32(1), truncation.max_terms, truncation.min_thresh
+    elseif truncation isa StochasticCoeffTruncation
+        kind, mn, seed = Int32(2), truncation.epsilon, rand(truncation.rng, UInt64)
+    elseif truncation isa StochasticSamplingTruncation
+        kind, mt, seed = Int32(3), truncation.n_keep, rand(truncation.rng, UInt64)
+    elseif !_is_compilable(truncation)
+        throw(ArgumentError("$(typeof(truncation)) has no GPU path (no CPU fallback)"))
+    end
     ket = Ref{W}(zero(W)); ce = Ref(0.0); cv = Ref(0.0); corr = Int32(0)
     if correction isa Union{EnergyCorrection,EnergyVarianceCorrection}
         corr = correction isa EnergyVarianceCorrection ? Int32(2) : Int32(1)
@@ -146,7 +156,7 @@ function PauliOperators.evolve!(v::CuSparsePauliVector{N,W}, gens::Vector{PauliB
                                 Base.unsafe_convert(Ptr{MergeFilter}, loc), kind, corr, mt, mn,
                                 Base.unsafe_convert(Ptr{W}, ket), Base.unsafe_convert(Ptr{Float64}, ce),
                                 C_NULL, Int32(-1), Int32(0), (0.0, 0.0, 0.0), C_NULL, C_NULL, 0, C_NULL,
-                                Int32(0), Int32(0), Base.unsafe_convert(Ptr{Float64}, cv)))
+                                Int32(0), Int32(0), Base.unsafe_convert(Ptr{Float64}, cv), seed))
         check(ccall((:pp_evolve, LIB), Cint,
                     (Ptr{Cvoid}, Ptr{W}, Ptr{W}, Ptr{Float64}, Ptr{Float64}, Int64, Ref{PPEvolveOpts}),
                     v.h, gz, gx, cs, sn, length(gens), opts))
@@ -190,6 +200,10 @@ function PauliOperators.truncate!(v::CuSparsePauliVector{N}, s::TruncationStrate
     before = corr isa EnergyCorrection ? expectation_value(v, corr.ψ) : 0.0
     if s isa AdaptiveTruncation
         _adaptive!(v, s)
+    elseif s isa StochasticCoeffTruncation
+        check(ccall((:pp_stochastic_clip, LIB), Cint, (Ptr{Cvoid}, Float64, UInt64), v.h, s.epsilon, rand(s.rng, UInt64)))
+    elseif s isa StochasticSamplingTruncation
+        check(ccall((:pp_stochastic_sample, LIB), Cint, (Ptr{Cvoid}, Int64, UInt64), v.h, s.n_keep, rand(s.rng, UInt64)))
     elseif s isa CompositeTruncation
         foreach(x -> PauliOperators.truncate!(v, x), s.strategies)
     elseif _is_compilable(s)
@@ -200,6 +214,10 @@ function PauliOperators.truncate!(v::CuSparsePauliVector{N}, s::TruncationStrate
     corr isa EnergyCorrection && (corr.accumulated_energy += expectation_value(v, corr.ψ) - before)
     return v
 end
+
+# stochastic_clip!(v, ε; rng) (spv_evolve.jl:35-52)
+PauliOperators.stochastic_clip!(v::CuSparsePauliVector, ε::Real; rng=Random.default_rng()) =
+    (check(ccall((:pp_stochastic_clip, LIB), Cint, (Ptr{Cvoid}, Float64, UInt64), v.h, ε, rand(rng, UInt64))); v)
 
 # channels (channels.jl:203-265)
 function _channel!(v::CuSparsePauliVector{N,W}, kind::Integer, prm, qubits) where {N,W}
