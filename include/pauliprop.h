@@ -258,6 +258,25 @@ int pp_stochastic_sample(pp_spv *h, int64_t n_keep, uint64_t seed);
  * pauli_channel! (203-221, 4).  prm: p, or pX,pY,pZ for kind 4.  qubit_mask: one
  * word (NULL = all qubits) as _spv_mask (channels.jl:200-201). */
 int pp_channel(pp_spv *h, int32_t kind, const double *prm, const void *qubit_mask);
+/* ---- SparsePauliVector algebra (spv_ops.jl) for real (Float64) coefficients. */
+/* mul!(v, a) (spv_ops.jl:12-17); with pp_copy it gives -v and v * a (:19-30). */
+int pp_scale(pp_spv *h, double a);
+/* norm(v, p) (spv_ops.jl:57-86): p = 2, 1, INFINITY, or any other p > 0. */
+int pp_norm(pp_spv *h, double p, double *out);
+/* tr(v) (spv_ops.jl:52-55): the identity coefficient times 2^N, where 2^N is the
+ * reference's Int64 power (it wraps: 0 for N >= 64). */
+int pp_trace(pp_spv *h, double *out);
+/* sum!(h, o) (spv_ops.jl:182-190) for sign = +1; h += -o for sign = -1 (with pp_copy:
+ * v1 + v2, v1 - v2, spv_ops.jl:131-167).  Unfiltered merge: zero sums are kept.
+ * o may be h. */
+int pp_sum(pp_spv *h, pp_spv *o, double sign);
+/* inner_product(a, b) (spv_ops.jl:378-399): sum over shared keys of c_a c_b. */
+int pp_inner_product(pp_spv *a, pp_spv *b, double *out);
+/* out = a * b (kind 0, spv_ops.jl:257-284), anticommutator!(out, a, b) (kind 1,
+ * :460-470) or commutator!(out, a, b) (kind 2, :446-458).  A real-typed product with
+ * an imaginary coefficient and every real commutator raise PP_ERROR_EXCEPTION, as the
+ * reference does.  out may be a or b; its previous contents are replaced. */
+int pp_product(pp_spv *out, pp_spv *a, pp_spv *b, int32_t kind);
 /* variance(v, ::Ket) (statistics.jl:6-22): <psi|O^2|psi> - <psi|O|psi>^2.  ket: one word. */
 int pp_variance(pp_spv *h, const void *ket, double *out);
 /* expectation_value(v, ::Ket) (spv_evolve.jl:133-134) -> _expectation_spv

@@ -24,6 +24,7 @@
 #include "kernels_batch.cuh"
 #include "kernels_learned.cuh"
 #include "kernels_stoch.cuh"
+#include "kernels_algebra.cuh"
 
 using namespace pp;
 
@@ -2056,4 +2057,208 @@ extern "C" int pp_stochastic_sample(pp_spv *h, int64_t n_keep, uint64_t seed) {
     if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
     if (n_keep < 0) return fail(PP_ARGUMENT_ERROR, "n_keep must be >= 0");
     return stoch_sample_apply(h, n_keep, seed);
+}
+
+// ------------------------------------------------------------------ SPV algebra (spv_ops.jl), real coefficients
+// Unfiltered merge of the handle's live set with the sorted run (VZ, VX, VC)[0, m)
+// as its appends: equal keys summed live first, zeros kept (_merge_spv!(v, m,
+// NOFILTER), spv_kernels.jl:326-386).
+template <int NW>
+static int merge_run(pp_spv *h, u64 *VZ, u64 *VX, double *VC, long long m) {
+    DevState st;
+    TRY(read_state(h, &st));
+    TRY(ensure_live(h, st.n + m));
+    DevParams *P = h->Ph;
+    compile_filter(nullptr, &P->strict);
+    P->corr_kind = 0;
+    P->chan_kind = -1;
+    TRY(upload_params(h));
+    TRY(read_state(h, &st));
+    st.an = m;
+    TRY(write_state(h, &st));
+    Bufs B = make_bufs(h);
+    B.vz = VZ;
+    B.vx = VX;
+    B.vc = VC;
+    launch_merge<NW, 1>(h, B, 0);
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    return check_err(h, st);
+}
+
+static int same_kind(pp_spv *a, pp_spv *b) {
+    if (!a || !b) return fail(PP_ARGUMENT_ERROR, "null handle");
+    if (a->N != b->N) return fail(PP_DIMENSION_MISMATCH, "operands have different qubit counts");
+    return PP_OK;
+}
+
+extern "C" int pp_scale(pp_spv *h, double a) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    DevState st;
+    TRY(read_state(h, &st));
+    if (st.n > 0) k_scale<<<h->nsm * 8, 256, 0, h->stream>>>(h->c[st.cur], st.n, a);
+    return sync_check(h);
+}
+
+extern "C" int pp_norm(pp_spv *h, double p, double *out) {
+    if (!h || !out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState st;
+    TRY(read_state(h, &st));
+    *out = 0.0;
+    if (st.n == 0) return PP_OK;
+    Scratch sc;
+    const int nb = std::min(4096, h->nsm * 8);
+    double *part, *res;
+    TRY(sc.get(&part, nb));
+    TRY(sc.get(&res, 1));
+    cudaStream_t s = h->stream;
+    const double *C = h->c[st.cur];
+    if (std::isinf(p)) {
+        k_absmax<<<nb, 256, 0, s>>>(C, st.n, part);
+        k_max_final<<<1, 32, 0, s>>>(part, nb, res);
+    } else {
+        double *val;
+        TRY(sc.get(&val, st.n));
+        k_norm_terms<<<h->nsm * 8, 256, 0, s>>>(C, st.n, p, val);
+        k_sum_partials<<<nb, 256, 0, s>>>(val, st.n, part);
+        k_expect_final<<<1, 32, 0, s>>>(part, nb, res);
+    }
+    double r = 0.0;
+    CU(cudaMemcpyAsync(&r, res, sizeof r, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    *out = std::isinf(p) ? r : p == 2.0 ? std::sqrt(r) : p == 1.0 ? r : std::pow(r, 1.0 / p);
+    return PP_OK;
+}
+
+extern "C" int pp_trace(pp_spv *h, double *out) {
+    if (!h || !out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState st;
+    TRY(read_state(h, &st));
+    // 2^N is the reference's Int64 power: it wraps for N >= 63
+    const double pow2 = h->N < 63 ? std::ldexp(1.0, h->N) : h->N == 63 ? -std::ldexp(1.0, 63) : 0.0;
+    *out = 0.0;
+    if (st.n == 0) return PP_OK;
+    u64 z[2] = {0, 0}, x[2] = {0, 0};
+    double c = 0.0;
+    CU(cudaMemcpyAsync(z, h->z[st.cur], h->NW * 8, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(x, h->x[st.cur], h->NW * 8, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(&c, h->c[st.cur], 8, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if ((z[0] | z[1] | x[0] | x[1]) == 0) *out = c * pow2;
+    return PP_OK;
+}
+
+extern "C" int pp_sum(pp_spv *h, pp_spv *o, double sign) {
+    TRY(same_kind(h, o));
+    if (sign != 1.0 && sign != -1.0) return fail(PP_ARGUMENT_ERROR, "sign must be +1 or -1");
+    DevState so, sh;
+    TRY(read_state(o, &so));
+    TRY(read_state(h, &sh));
+    if (sh.an != 0) return fail(PP_ERROR_EXCEPTION, "sum! on a SparsePauliVector with pending appends");
+    const long long m = so.n;
+    if (m == 0) return PP_OK;
+    TRY(ensure_append(h, std::max(m, h->acap_phys), 0));
+    TRY(cudaStreamSynchronize(o->stream) == cudaSuccess ? PP_OK : fail(PP_DEVICE_ERROR, "stream"));
+    k_copy_terms<<<h->nsm * 8, 256, 0, h->stream>>>(o->z[so.cur], o->x[so.cur], o->c[so.cur], m, h->NW, sign, h->az,
+                                                     h->ax, h->ac);
+    return h->NW == 1 ? merge_run<1>(h, h->az, h->ax, h->ac, m) : merge_run<2>(h, h->az, h->ax, h->ac, m);
+}
+
+extern "C" int pp_inner_product(pp_spv *a, pp_spv *b, double *out) {
+    TRY(same_kind(a, b));
+    if (!out) return fail(PP_ARGUMENT_ERROR, "null argument");
+    DevState sa, sb;
+    TRY(read_state(a, &sa));
+    TRY(read_state(b, &sb));
+    *out = 0.0;
+    if (sa.n == 0 || sb.n == 0) return PP_OK;
+    CU(cudaStreamSynchronize(b->stream));
+    Scratch sc;
+    const int nb = std::min(4096, a->nsm * 8);
+    double *val, *part, *res;
+    TRY(sc.get(&val, sa.n));
+    TRY(sc.get(&part, nb));
+    TRY(sc.get(&res, 1));
+    cudaStream_t s = a->stream;
+    if (a->NW == 1)
+        k_inner_terms<1><<<a->nsm * 8, 256, 0, s>>>(a->z[sa.cur], a->x[sa.cur], a->c[sa.cur], sa.n, b->z[sb.cur],
+                                                     b->x[sb.cur], b->c[sb.cur], sb.n, val);
+    else
+        k_inner_terms<2><<<a->nsm * 8, 256, 0, s>>>(a->z[sa.cur], a->x[sa.cur], a->c[sa.cur], sa.n, b->z[sb.cur],
+                                                     b->x[sb.cur], b->c[sb.cur], sb.n, val);
+    k_sum_partials<<<nb, 256, 0, s>>>(val, sa.n, part);
+    k_expect_final<<<1, 32, 0, s>>>(part, nb, res);
+    CU(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, s));
+    return sync_check(a);
+}
+
+template <int NW>
+static int product_nw(pp_spv *out, pp_spv *a, pp_spv *b, int kind) {
+    DevState sa, sb;
+    TRY(read_state(a, &sa));
+    TRY(read_state(b, &sb));
+    const long long tot = sa.n * sb.n;
+    if (tot > 0x7fffffffll - 8192) return fail(PP_OUT_OF_MEMORY, "more than 2^31 term pairs");
+    CU(cudaStreamSynchronize(a->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    TRY(ensure_append(out, std::max(tot, out->acap_phys), 0));
+    Scratch sc;
+    unsigned char *keep;
+    int *err;
+    TRY(sc.get(&keep, tot));
+    TRY(sc.get(&err, 1));
+    cudaStream_t s = out->stream;
+    CU(cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (tot > 0)
+        k_pairs<NW><<<out->nsm * 8, 256, 0, s>>>(a->z[sa.cur], a->x[sa.cur], a->c[sa.cur], sa.n, b->z[sb.cur],
+                                                  b->x[sb.cur], b->c[sb.cur], sb.n, kind, out->az, out->ax, out->ac,
+                                                  keep, err);
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (e) return fail(PP_ERROR_EXCEPTION, "InexactError: the product has imaginary coefficients; "
+                                           "use a complex coefficient type");
+    // keep the surviving pairs in generation order (anticommutator), then sort stably by key
+    u64 *PZ = out->az, *PX = out->ax;
+    double *PC = out->ac;
+    long long m = tot;
+    if (kind == 1 && tot > 0) {
+        const long long ntiles = (tot + FC_TILE - 1) / FC_TILE;
+        int *cnt, *off;
+        long long *total;
+        TRY(sc.get(&cnt, ntiles));
+        TRY(sc.get(&off, ntiles));
+        TRY(sc.get(&total, 1));
+        const int g = (int)std::min<long long>(ntiles, 8ll * out->nsm);
+        k_flag_count<<<g, FC_THREADS, 0, s>>>(keep, tot, cnt);
+        k_flag_scan<<<1, 1024, 0, s>>>(ntiles, cnt, off, total);
+        k_flag_write<<<g, FC_THREADS, 0, s>>>(keep, tot, off, out->az, out->ax, out->ac, nullptr, NW, nullptr, out->tz,
+                                              out->tx, out->tc);
+        CU(cudaMemcpyAsync(&m, total, sizeof m, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        PZ = out->tz; PX = out->tx; PC = out->tc;
+    }
+    int in_t = 0;
+    u64 *QZ = PZ == out->az ? out->tz : out->az, *QX = PX == out->ax ? out->tx : out->ax;
+    double *QC = PC == out->ac ? out->tc : out->ac;
+    TRY(radix_sort<NW>(out, PZ, PX, PC, QZ, QX, QC, m, &in_t));
+    if (in_t) { PZ = QZ; PX = QX; PC = QC; }
+    // result = the sorted triples summed by key (_triples_to_live!, spv_ops.jl:234-255)
+    DevState so;
+    TRY(read_state(out, &so));
+    so.n = 0;
+    so.an = 0;
+    so.seg_dense = 1;
+    TRY(write_state(out, &so));
+    return merge_run<NW>(out, PZ, PX, PC, m);
+}
+
+extern "C" int pp_product(pp_spv *out, pp_spv *a, pp_spv *b, int32_t kind) {
+    TRY(same_kind(a, b));
+    TRY(same_kind(out, a));
+    if (kind < 0 || kind > 2) return fail(PP_ARGUMENT_ERROR, "kind: 0 product, 1 anticommutator, 2 commutator");
+    if (kind == 2)
+        return fail(PP_ERROR_EXCEPTION, "commutator coefficients are imaginary; use a complex coefficient type "
+                                        "(T=ComplexF64)");
+    return out->NW == 1 ? product_nw<1>(out, a, b, kind) : product_nw<2>(out, a, b, kind);
 }

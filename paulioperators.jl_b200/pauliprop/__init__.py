@@ -13,7 +13,8 @@ from .truncation import (NOFILTER, AdaptiveTruncation, CoeffTruncation, Composit
                          TruncationStrategy, WeightDampedTruncation, WeightTruncation,
                          XWeightDampedTruncation, XWeightTruncation, combine_filters,
                          compile_filter, is_compilable)
-from .spv import (SparsePauliVector, WindowCounters, bit_flip_channel, bit_flip_channel_,
+from .spv import (SparsePauliVector, WindowCounters, add, anticommutator, anticommutator_, commutator,
+                  commutator_, inner_product, mul_, norm, product, scaled, sub, sum_, tr, bit_flip_channel, bit_flip_channel_,
                   bit_phase_flip_channel, bit_phase_flip_channel_, check_spv, clip_,
                   coeff_clip_, dephasing_channel, dephasing_channel_, depolarizing_channel,
                   depolarizing_channel_, depolarizing_p_for_weight_decay, evolve, evolve_,

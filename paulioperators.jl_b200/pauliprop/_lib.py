@@ -131,6 +131,12 @@ SIGNATURES = {
                                       POINTER(PPDropSample)]),
     "pp_sample_terms": (c_int32, [c_void_p, c_int32, c_double, c_double, c_int64, c_uint64, c_void_p, c_void_p,
                                   c_void_p, c_int64, POINTER(c_int64)]),
+    "pp_scale": (c_int32, [c_void_p, c_double]),
+    "pp_norm": (c_int32, [c_void_p, c_double, POINTER(c_double)]),
+    "pp_trace": (c_int32, [c_void_p, POINTER(c_double)]),
+    "pp_sum": (c_int32, [c_void_p, c_void_p, c_double]),
+    "pp_inner_product": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
+    "pp_product": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32]),
     "pp_last_error": (c_char_p, []),
 }
 

@@ -142,6 +142,24 @@ class SparsePauliVector:
         o.N, o.nw, o._h = self.N, self.nw, h
         return o
 
+    # -- algebra (spv_ops.jl) ----------------------------------------------------
+    def __neg__(self):
+        return scaled(self, -1.0)
+
+    def __add__(self, other):
+        return add(self, other)
+
+    def __sub__(self, other):
+        return sub(self, other)
+
+    def __mul__(self, other):
+        if isinstance(other, SparsePauliVector):
+            return product(self, other)
+        return scaled(self, other)
+
+    def __rmul__(self, a):
+        return scaled(self, a)
+
     def device_bytes(self):
         b = c_int64()
         check(lib.pp_device_bytes(self._h, byref(b)))
@@ -451,6 +469,90 @@ def variance(v, ket):
     out = c_double()
     check(lib.pp_variance(v._h, _ptr(k), byref(out)))
     return out.value
+
+
+# ----------------------------------------------------------------------------- algebra
+def mul_(v, a):
+    """mul!(v, a) (spv_ops.jl:12-17): v.c *= a."""
+    check(lib.pp_scale(v._h, float(a)))
+    return v
+
+
+def scaled(v, a):
+    """v * a, a * v, -v (spv_ops.jl:19-30)."""
+    return mul_(v.copy(), a)
+
+
+def norm(v, p=2):
+    """norm(v, p) (spv_ops.jl:57-86) for p = 2, 1, inf or any p > 0."""
+    out = c_double()
+    check(lib.pp_norm(v._h, float(p), byref(out)))
+    return out.value
+
+
+def tr(v):
+    """tr(v) (spv_ops.jl:52-55): the identity coefficient times 2^N, with the
+    reference's Int64 power (0 for N >= 64)."""
+    out = c_double()
+    check(lib.pp_trace(v._h, byref(out)))
+    return out.value
+
+
+def sum_(v1, v2):
+    """sum!(v1, v2) (spv_ops.jl:182-190): v1 += v2 by an unfiltered merge."""
+    check(lib.pp_sum(v1._h, v2._h, 1.0))
+    return v1
+
+
+def add(v1, v2):
+    """v1 + v2 (spv_ops.jl:131-165); zero sums are kept."""
+    return sum_(v1.copy(), v2)
+
+
+def sub(v1, v2):
+    """v1 - v2 (spv_ops.jl:167)."""
+    out = v1.copy()
+    check(lib.pp_sum(out._h, v2._h, -1.0))
+    return out
+
+
+def inner_product(v1, v2):
+    """inner_product(v1, v2) (spv_ops.jl:378-399): Σ over shared keys of c1·c2."""
+    out = c_double()
+    check(lib.pp_inner_product(v1._h, v2._h, byref(out)))
+    return out.value
+
+
+def _product_into(out, a, b, kind):
+    check(lib.pp_product(out._h, a._h, b._h, kind))
+    return out
+
+
+def product(a, b):
+    """a * b (spv_ops.jl:257-284); raises for an imaginary coefficient, as the
+    reference's real-typed product does (InexactError)."""
+    return _product_into(SparsePauliVector(a.N, 16, 16), a, b, 0)
+
+
+def anticommutator_(out, a, b):
+    """anticommutator!(out, A, B) (spv_ops.jl:460-470): {A, B} into out."""
+    return _product_into(out, a, b, 1)
+
+
+def anticommutator(a, b):
+    """anticommutator(A, B) (spv_ops.jl:479-485)."""
+    return anticommutator_(SparsePauliVector(a.N, 16, 16), a, b)
+
+
+def commutator_(out, a, b):
+    """commutator!(out, A, B) (spv_ops.jl:446-458): its coefficients are imaginary, so
+    it raises for real (Float64) vectors, as the reference does."""
+    return _product_into(out, a, b, 2)
+
+
+def commutator(a, b):
+    """commutator(A, B) (spv_ops.jl:472-477)."""
+    return commutator_(SparsePauliVector(a.N, 16, 16), a, b)
 
 
 def check_spv(v):
