@@ -9,6 +9,7 @@
 module PauliOperatorsGPU
 
 using PauliOperators
+using LinearAlgebra
 using Random
 using PauliOperators: MergeFilter, NOFILTER, _compile_filter, _is_compilable, _pack, _unpack, _word_type,
                       CorrectionAccumulator, NoCorrection, EnergyCorrection, EnergyVarianceCorrection,
@@ -76,6 +77,12 @@ mutable struct CuSparsePauliVector{N,W<:Unsigned}
         r = Ref{Ptr{Cvoid}}(C_NULL)
         check(ccall((:pp_create, LIB), Cint, (Int32, Int64, Int64, Ref{Ptr{Cvoid}}), N, live_cap, append_cap, r))
         v = new{N,W}(r[])
+        finalizer(x -> ccall((:pp_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), v)
+        return v
+    end
+    # wrap an existing handle (pp_copy)
+    function CuSparsePauliVector{N,W}(h::Ptr{Cvoid}) where {N,W}
+        v = new{N,W}(h)
         finalizer(x -> ccall((:pp_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), v)
         return v
     end
@@ -247,6 +254,47 @@ function check_spv(v::CuSparsePauliVector)
     ok[] == 1 || error("live keys not strictly increasing")
     return true
 end
+
+# SparsePauliVector algebra (spv_ops.jl), real coefficients
+function Base.copy(v::CuSparsePauliVector{N,W}) where {N,W}
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:pp_copy, LIB), Cint, (Ptr{Cvoid}, Ref{Ptr{Cvoid}}), v.h, r))
+    o = CuSparsePauliVector{N,W}(r[])
+    return o
+end
+LinearAlgebra.mul!(v::CuSparsePauliVector, a::Real) =
+    (check(ccall((:pp_scale, LIB), Cint, (Ptr{Cvoid}, Float64), v.h, a)); v)
+Base.:*(v::CuSparsePauliVector, a::Real) = mul!(copy(v), a)
+Base.:*(a::Real, v::CuSparsePauliVector) = v * a
+Base.:-(v::CuSparsePauliVector) = v * -1
+function LinearAlgebra.norm(v::CuSparsePauliVector, p::Real=2)
+    out = Ref(0.0)
+    check(ccall((:pp_norm, LIB), Cint, (Ptr{Cvoid}, Float64, Ref{Float64}), v.h, p, out))
+    return out[]
+end
+function LinearAlgebra.tr(v::CuSparsePauliVector)
+    out = Ref(0.0)
+    check(ccall((:pp_trace, LIB), Cint, (Ptr{Cvoid}, Ref{Float64}), v.h, out))
+    return out[]
+end
+Base.sum!(v1::CuSparsePauliVector{N}, v2::CuSparsePauliVector{N}) where {N} =
+    (check(ccall((:pp_sum, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64), v1.h, v2.h, 1.0)); v1)
+Base.:+(v1::CuSparsePauliVector{N}, v2::CuSparsePauliVector{N}) where {N} = sum!(copy(v1), v2)
+Base.:-(v1::CuSparsePauliVector{N}, v2::CuSparsePauliVector{N}) where {N} =
+    (o = copy(v1); check(ccall((:pp_sum, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64), o.h, v2.h, -1.0)); o)
+function PauliOperators.inner_product(v1::CuSparsePauliVector{N}, v2::CuSparsePauliVector{N}) where {N}
+    out = Ref(0.0)
+    check(ccall((:pp_inner_product, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ref{Float64}), v1.h, v2.h, out))
+    return out[]
+end
+_product!(out::CuSparsePauliVector, A::CuSparsePauliVector, B::CuSparsePauliVector, kind) =
+    (check(ccall((:pp_product, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int32), out.h, A.h, B.h, kind)); out)
+Base.:*(A::CuSparsePauliVector{N,W}, B::CuSparsePauliVector{N,W}) where {N,W} =
+    _product!(CuSparsePauliVector{N,W}(16, 16), A, B, 0)
+PauliOperators.anticommutator!(out::CuSparsePauliVector, A::CuSparsePauliVector, B::CuSparsePauliVector) =
+    _product!(out, A, B, 1)
+PauliOperators.commutator!(out::CuSparsePauliVector, A::CuSparsePauliVector, B::CuSparsePauliVector) =
+    _product!(out, A, B, 2)
 
 export CuSparsePauliVector, check_spv
 
