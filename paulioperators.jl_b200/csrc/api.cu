@@ -480,6 +480,14 @@ static int launch_setup(pp_spv *h) {
     CU(cudaFuncSetAttribute(k_tilescan<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tilescan_smem<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    if (NW == 2) {
+        // two merge CTAs per SM need the largest shared-memory carveout (2 x 113 KB);
+        // N <= 64 leaves the split to the driver (more L1 for the merge's gathers)
+        const int mx = (int)cudaSharedmemCarveoutMaxShared;
+        CU(cudaFuncSetAttribute(k_merge<NW, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, mx));
+        CU(cudaFuncSetAttribute(k_merge<NW, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, mx));
+        CU(cudaFuncSetAttribute(k_merge<NW, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, mx));
+    }
     int occ = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_classify<NW>, A_THREADS, 2 * NW * A_TILE * 8 + A_TILE));
     h->occA1 = std::max(1, occ);

@@ -973,7 +973,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     __shared__ int s_sc[B_THREADS / 32 + 1];
     __shared__ double s_red[3][B_THREADS / 32];
     __shared__ unsigned s_base;
-    __shared__ double s_expw[130], s_expxw[130], s_ch[3][130];
+    __shared__ double s_expw[130], s_expxw[130];   // filter tables; the channel tables are read through L1
     __shared__ int s_so[B_SEGL], s_sp[B_SEGL];   // live segment list of the tile (MODE 0)
     extern __shared__ u64 sm[];
     u64 *skz = sm;                                                    // [NW][B_CAP]
@@ -998,9 +998,6 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
     const bool do_meas = (flags & GEN_MEASURE) != 0 || do_corr;
     const int chan_kind = P.chan_kind;
     const u64 chan_mask[2] = {P.chan_mask[0], P.chan_mask[1]};
-    if (do_chan) {
-        for (int i = tid; i < 130; i += B_THREADS) { s_ch[0][i] = P.chanX[i]; s_ch[1][i] = P.chanY[i]; s_ch[2][i] = P.chanZ[i]; }
-    }
     FLite fs;                       // early-merge pre-filter (the strict filter of the evolve call)
     if constexpr (MODE == 0) fs = flite(P.strict);
     const long long n = S->n, a = v_count<MODE>(S), tot = n + a;
@@ -1194,7 +1191,7 @@ __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
             }
             if (harvest && fin) continue;
             const bool ch = do_chan && !fin;
-            const double o = ch ? __dmul_rn(acc, chan_lite<NW>(chan_kind, chan_mask, s_ch[0], s_ch[1], s_ch[2], kp)) : acc;
+            const double o = ch ? __dmul_rn(acc, chan_lite<NW>(chan_kind, chan_mask, P.chanX, P.chanY, P.chanZ, kp)) : acc;
             if (diag && do_meas) e_keep.add(sgn * o);
             outq[q] = o;
             slotq[q] = (unsigned short)sl;
