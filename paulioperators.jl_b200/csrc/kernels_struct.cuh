@@ -127,7 +127,7 @@ __device__ __forceinline__ bool term_finished(const Bufs &B, long long rot, cons
 // that emit a sin branch, their h levels and the tile aggregates.  srcidx holds
 // the physical index of each emitting term (used by the merge's gather).
 template <int NW>
-__global__ void __launch_bounds__(A_THREADS) k_classify(Bufs B) {
+__global__ void __launch_bounds__(A_THREADS, 2) k_classify(Bufs B) {
     DevState *S = B.S;
     if (S->err) return;
     const long long rot = S->rot;
