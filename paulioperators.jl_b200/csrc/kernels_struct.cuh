@@ -883,7 +883,7 @@ __global__ void __launch_bounds__(P_THREADS) k_partition(Bufs B) {
 }
 
 // ---------------------------------------------------------------- B merge
-constexpr int B_VPT = B_CAP / B_THREADS;   // staged inputs per thread (10)
+constexpr int B_VPT = B_CAP / B_THREADS;   // staged inputs per thread (5)
 constexpr int B_HALF = B_VPT;              // loads issued in one batch per tile
 constexpr int B_SEGL = 256;                // live segments of a tile held in shared memory
 
@@ -959,9 +959,10 @@ __device__ __forceinline__ double chan_lite(int kind, const u64 *mask, const dou
 }
 
 // One merge tile: the merge-path diagonal range [split[t], split[t+1]) of
-// (live, appended).  Each CTA loops over tiles taken in order from a counter;
-// while warp 0 resolves the tile's output offset by decoupled look-back, the
-// other warps already issue the next tile's global loads into registers.
+// (live, appended).  Each CTA loops over tiles taken in order from a counter.
+// A window-1 merge (MODE 0) writes each tile to its own SEG-term slot; the
+// general merges (MODE 1, 2) find the tile's output offset by decoupled look-back
+// in warp 0.
 
 template <int NW, int MODE>
 __global__ void __launch_bounds__(B_THREADS, 2) k_merge(Bufs B, int argflags) {
