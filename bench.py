@@ -168,13 +168,42 @@ def reduce_sum(x, ws, device=None):
 
 
 # ----------------------------------------------------------------------------- CPU legs
+def _oracle_full_run(w):
+    """The whole circuit of a workload with at most SNAP_LAYER layers on the CPU
+    oracle, from the observable, one Trotter layer (and its channel) at a time.
+    Returns (terms_in, seconds, final oracle vector)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    import pauliprop as pp
+    f = tuple(pp.compile_filter(strategy_of(w)))
+    kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
+    gens = [(p.z, p.x) for p in w.layer]
+    v = orc.OracleSPV.from_terms(w.N, w.observable)
+    terms, dt = 0, 0.0
+    for _ in range(w.layers):
+        n0 = len(v)
+        t0 = time.perf_counter()
+        _, ctr = v.evolve(gens, w.angles, window=1, strict=f, nwin=len(gens))
+        if kind is not None:
+            v.channel(kind, [w.channel[1]])
+        dt += time.perf_counter() - t0
+        terms += n0 + int(ctr[2][:-1].sum())
+    return terms, dt, v
+
+
 def _oracle_layer_sample(wname, snap_layer, reps, q=None):
     """Worker: build the snap_layer state on the CPU oracle, then time `reps` evolutions of
-    the next layer from copies of it.  Returns [(terms_in, seconds), ...]."""
+    the next layer from copies of it; a circuit of at most snap_layer layers is timed
+    whole, end to end, `reps` times.  Returns [(terms_in, seconds), ...]."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
     import pauliprop as pp
     w = workload(wname)
+    if w.layers <= snap_layer:
+        out = [_oracle_full_run(w)[:2] for _ in range(reps)]
+        if q is not None:
+            q.put(out)
+        return out
     f = tuple(pp.compile_filter(strategy_of(w)))
     kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
     v = orc.OracleSPV.from_terms(w.N, w.observable)
@@ -248,17 +277,21 @@ def run_reference(args):
     value = statistics.median(per_step)
     w = workload(args.workload)
     terms_in = res[0][args.warmup][0]
+    whole = w.layers <= SNAP_LAYER
+    what = (f"{w.name} end to end ({w.layers} layers x {len(w.layer)} rotations from the observable)" if whole
+            else f"{w.name} layer {SNAP_LAYER + 1} from the layer-{SNAP_LAYER} state")
     line = {
         "metric": "terms/s rotate+merge+clip", "value": value, "unit": "terms/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * terms_in / (value / nthreads), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded circuit)", "impl": "reference",
-        "config": {"workload": f"{w.name} layer {SNAP_LAYER + 1} from the layer-{SNAP_LAYER} state",
-                   "N": w.N, "rotations_per_sample": len(w.layer), "threads": nthreads},
+        "config": {"workload": what, "N": w.N,
+                   "rotations_per_sample": len(w.layer) * (w.layers if whole else 1), "threads": nthreads},
         "cpu_baseline": {"value": value, "unit": "terms/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{w.name}: one Trotter layer ({len(w.layer)} rotations + channel) "
-                                   f"from the layer-{SNAP_LAYER} state, per worker process"},
+                         "sample": (f"{what}, per worker process" if whole else
+                                    f"{w.name}: one Trotter layer ({len(w.layer)} rotations + channel) "
+                                    f"from the layer-{SNAP_LAYER} state, per worker process")},
         "e2e": {"value": value, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -634,6 +667,20 @@ def run_ours(args):
 
     # CPU baseline on an identical snapshot (rank 0 at N=1)
     cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and w.layers <= SNAP_LAYER:
+        # a circuit this short is timed end to end on the oracle, and the GPU's
+        # final term set is checked against the oracle's
+        ti_cpu, dt_cpu, vorc = _oracle_full_run(w)
+        upload_dev()
+        pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0)
+        gz_, gx_, gc_ = g.to_arrays()
+        oz_, ox_, oc_ = vorc.arrays()
+        same = bool(np.array_equal(gz_, oz_) and np.array_equal(gx_, ox_)
+                    and np.abs(gc_ - oc_).max(initial=0.0) <= 1e-12 * max(1.0, np.abs(oc_).max(initial=1.0)))
+        cpu = {"value": ti_cpu / dt_cpu, "unit": "terms/s", "cores": 1, "kind": "port",
+               "sample": f"{w.name} end to end ({w.layers} layers x {per} rotations from the observable), "
+                         f"C restatement of the reference path, 1 thread",
+               "gpu_matches_oracle_on_sample": same}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and w.layers > SNAP_LAYER:
         upload_dev()
         pp.evolve_(g, w.layer * SNAP_LAYER, w.angles * SNAP_LAYER, truncation=strat, channel=ch,

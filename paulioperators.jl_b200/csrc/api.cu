@@ -25,6 +25,7 @@
 #include "kernels_learned.cuh"
 #include "kernels_stoch.cuh"
 #include "kernels_algebra.cuh"
+#include "kernels_small.cuh"
 
 using namespace pp;
 
@@ -480,6 +481,7 @@ static int launch_setup(pp_spv *h) {
     CU(cudaFuncSetAttribute(k_tilescan<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tilescan_smem<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
     CU(cudaFuncSetAttribute(k_merge<NW, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem_bytes<NW>()));
+    CU(cudaFuncSetAttribute(k_small_run<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem<NW>()));
     if (NW == 2) {
         // two merge CTAs per SM need the largest shared-memory carveout (2 x 113 KB);
         // N <= 64 leaves the split to the driver (more L1 for the merge's gathers)
@@ -738,14 +740,38 @@ struct RunProf {
 
 // Structured window-1 sequence over rotations [start, L) (the device cursor
 // S->rot is at start): chunks of CHUNK_ROT rotations between state read-backs; on
-// ERR_OVERFLOW grow and resume at the rotation that stopped.
+// ERR_OVERFLOW grow and resume at the rotation that stopped.  While the live set
+// fits k_small_run's shared memory (and the call has no local truncation,
+// correction or batched instances, and no per-rotation timing), one launch of it
+// runs the rotations instead.
 template <int NW>
 static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof) {
     long long done = start;
     const bool timed = prof->on || (ctr && (ctr->t_rotate || ctr->t_merge));
     std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
     bool table = false;            // the device segment table describes the (dense) live set
+    const bool small_ok = !timed && !h->batch_on && !h->Ph->local_active && h->Ph->corr_kind == 0;
+    long long ncur = small_cap<NW>() + 1;   // live terms at the chunk's start (read when small_ok)
+    if (small_ok) {
+        DevState st;
+        TRY(read_state(h, &st));
+        ncur = st.n;
+    }
     while (done < L) {
+        if (small_ok && ncur <= small_cap<NW>()) {
+            Bufs B = make_bufs(h);
+            k_small_run<NW><<<1, SM_THREADS, small_smem<NW>(), h->stream>>>(B);
+            prof->launches += 1;
+            TRY(sync_check(h));
+            DevState st;
+            TRY(read_state(h, &st));
+            if (st.err) { ensure_dense(h); return check_err(h, st); }
+            table = false;
+            ncur = st.n;
+            if (st.rot == done) ncur = small_cap<NW>() + 1;   // no progress: leave it to the multi-kernel path
+            done = st.rot;
+            continue;
+        }
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
@@ -788,6 +814,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
         TRY(sync_check(h));
         DevState st;
         TRY(read_state(h, &st));
+        ncur = st.n;
         if (timed) {
             // rotations that ran are [done, st.rot); the rest were no-ops
             const long long base = (long long)ev.size() / 5 - (end - done);
