@@ -376,6 +376,53 @@ def test_growth_from_tiny_capacity():
     compare(g, v, bitexact=True)
 
 
+def random_rotations(rng, N, count, lo, hi):
+    gens, angs = [], []
+    for _ in range(count):
+        i, j = rng.sample(range(N), 2)
+        gens.append(((1 << i) | (1 << j), 0) if rng.random() < 0.5 else (0, 1 << i))
+        angs.append(rng.uniform(lo, hi))
+    return gens, angs
+
+
+def test_growth_overflow_multikernel():
+    """A set above the single-CTA capacity grows 3000 -> ~8e4 terms within one chunk
+    of rotations from a one-term capacity: the multi-kernel path flags the overflow,
+    the host grows the buffers and resumes, with an unchanged result."""
+    rng = random.Random(64)
+    N = 64
+    terms = {}
+    while len(terms) < 3000:
+        terms[(rng.getrandbits(N), rng.getrandbits(N))] = rng.uniform(-1.0, 1.0)
+    v = oracle_from_terms(N, terms)
+    g = pp.SparsePauliVector(N, 1, v.append_cap)
+    g.upload(*v.arrays(), sorted=True)
+    gens, angs = random_rotations(rng, N, 8, 0.1, 1.0)
+    v.evolve(gens, angs, window=1, strict=filt(("coeff", 1e-6)))
+    pp.evolve_(g, [pp.PauliBasis(N, z, x) for z, x in gens], angs, truncation=strategy(("coeff", 1e-6)))
+    assert len(g) > 50000
+    compare(g, v, bitexact=True)
+
+
+@pytest.mark.parametrize("N,n0,thresh", [(64, 3000, 0.2), (100, 1500, 0.25)])
+def test_shrink_into_single_cta_path(N, n0, thresh):
+    """The live set starts above the single-CTA capacity (2048 terms for N <= 64,
+    1024 above) and a strong threshold shrinks it below within the first 64-rotation
+    chunk: the next chunk runs in the single-CTA kernel, which reads the segment
+    table the multi-kernel merge left.  Bit-exact against the oracle."""
+    rng = random.Random(7)
+    terms = {}
+    while len(terms) < n0:
+        terms[(rng.getrandbits(N), rng.getrandbits(N))] = rng.uniform(-1.0, 1.0)
+    v = oracle_from_terms(N, terms)
+    g = gpu_from_oracle(v, N)
+    gens, angs = random_rotations(rng, N, 100, 0.05, 0.3)
+    v.evolve(gens, angs, window=1, strict=filt(("coeff", thresh)))
+    pp.evolve_(g, [pp.PauliBasis(N, z, x) for z, x in gens], angs, truncation=strategy(("coeff", thresh)))
+    assert 0 < len(g) < (2048 if N <= 64 else 1024)
+    compare(g, v, bitexact=True)
+
+
 def test_copy_and_nonmutating():
     rng = random.Random(9)
     terms = rand_terms(rng, 8, 50)
