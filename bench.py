@@ -16,9 +16,15 @@ Arms:
                     buffers (pinned upload, evolve, download of the final term
                     set and the expectation value) timed by the host clock.
   --impl reference  the reference algorithm on the host cores: the C restatement
-                    of the reference's CPU path (oracle/, "port"), one worker
-                    process per host thread, each timing one Trotter layer from
-                    the layer-10 state (a bounded sample of the same workload).
+                    of the reference's CPU path (oracle/, "port").  Each step is
+                    one whole-circuit run from the observable; the K steps run
+                    in min(K, host threads) concurrent single-threaded worker
+                    processes, and `value` is their aggregate terms/s.  The
+                    workers never load libpauliprop.so.
+The GPU arm also runs the whole circuit once on the oracle (1 thread, in a
+spawned process while the GPU is timed): that is its `cpu_baseline`, and the
+GPU's final term set and expectation value are checked against it
+(`final_check`).
 --workload batch256: 256 uneven instances of the 8x8 lattice in one batched pass
 (pp_evolve_batch): depth U{4..24} layers, θ_J, θ_h ~ U[0.05, 0.5], observable a
 random Pauli string of weight 1-4, CoeffTruncation(1e-4), no noise.  One step =
@@ -52,10 +58,8 @@ BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
 # DRAM traffic of k_merge<1,0> per algorithmic byte, from one ncu capture of the 176
 # merge launches of layer 11 of this workload (dram__bytes_read.sum +
 # dram__bytes_write.sum = 115.1 MB per launch against B(n + a + m) = 150.9 MB:
-# the gathered sin branches re-read live terms that are still in L2); the
-# summary and its command are in profiles/k_merge_lattice64_layer11.md
+# the gathered sin branches re-read live terms that are still in L2)
 MERGE_TRAFFIC_PER_ALG_BYTE = 115.09 / 150.88
-SNAP_LAYER = 10                      # CPU-baseline sample: layer 11 from the layer-10 state
 
 
 def parse():
@@ -168,83 +172,75 @@ def reduce_sum(x, ws, device=None):
 
 
 # ----------------------------------------------------------------------------- CPU legs
-def _oracle_full_run(w):
-    """The whole circuit of a workload with at most SNAP_LAYER layers on the CPU
-    oracle, from the observable, one Trotter layer (and its channel) at a time.
-    Returns (terms_in, seconds, final oracle vector)."""
+# The CPU legs run the C restatement of the reference path (oracle/liborc.so) in
+# processes that import only the library-free host modules of pauliprop
+# (circuits, truncation, paulis): libpauliprop.so is never mapped into them.
+def _native_libs_loaded():
+    """Shared objects of this repository mapped into the calling process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                p = line.split()[-1] if line.strip() else ""
+                if p.endswith(".so") and p.startswith(ROOT):
+                    out.add(os.path.relpath(p, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def _oracle_whole_circuit(wname, layers=None, out_path=None):
+    """The whole circuit of a workload on the CPU oracle, from the observable, one
+    evolve! call per Trotter layer followed by the layer's channel (the
+    reference's usage: spv_evolve.jl:312-387, channels.jl:223-243).
+    Returns dict(terms_in, seconds, expect, n, libs); with out_path the final term
+    set is saved there (npz: z, x, c)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
     import orc
-    import pauliprop as pp
-    f = tuple(pp.compile_filter(strategy_of(w)))
+    from pauliprop import circuits
+    from pauliprop.truncation import CoeffTruncation, CompositeTruncation, WeightTruncation, compile_filter
+    w = {"lattice64": circuits.lattice64, "chain20": circuits.chain20,
+         "graph127": circuits.random_graph127}[wname]()
+    parts = [CoeffTruncation(w.thresh)] + ([WeightTruncation(w.wmax)] if w.wmax else [])
+    f = tuple(compile_filter(CompositeTruncation(*parts)))
     kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
     gens = [(p.z, p.x) for p in w.layer]
     v = orc.OracleSPV.from_terms(w.N, w.observable)
     terms, dt = 0, 0.0
-    for _ in range(w.layers):
+    for _ in range(w.layers if layers is None else layers):
         n0 = len(v)
         t0 = time.perf_counter()
         _, ctr = v.evolve(gens, w.angles, window=1, strict=f, nwin=len(gens))
         if kind is not None:
             v.channel(kind, [w.channel[1]])
         dt += time.perf_counter() - t0
+        # terms entering each rotation: n0, then the live count after each merge
         terms += n0 + int(ctr[2][:-1].sum())
-    return terms, dt, v
+    res = {"terms_in": terms, "seconds": dt, "expect": v.expect(0), "n": len(v), "libs": _native_libs_loaded()}
+    if out_path:
+        z, x, c = v.arrays()
+        np.savez(out_path, z=z, x=x, c=c)
+    return res
 
 
-def _oracle_layer_sample(wname, snap_layer, reps, q=None):
-    """Worker: build the snap_layer state on the CPU oracle, then time `reps` evolutions of
-    the next layer from copies of it; a circuit of at most snap_layer layers is timed
-    whole, end to end, `reps` times.  Returns [(terms_in, seconds), ...]."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import orc
-    import pauliprop as pp
-    w = workload(wname)
-    if w.layers <= snap_layer:
-        out = [_oracle_full_run(w)[:2] for _ in range(reps)]
-        if q is not None:
-            q.put(out)
-        return out
-    f = tuple(pp.compile_filter(strategy_of(w)))
-    kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
-    v = orc.OracleSPV.from_terms(w.N, w.observable)
-    gens = [(p.z, p.x) for p in w.layer]
-    for _ in range(snap_layer):
-        v.evolve(gens, w.angles, window=1, strict=f)
-        if kind is not None:
-            v.channel(kind, [w.channel[1]])
-    out = []
-    for _ in range(reps):
-        s = v.copy()
-        n0 = len(s)
-        t0 = time.perf_counter()
-        _, ctr = s.evolve(gens, w.angles, window=1, strict=f, nwin=len(gens))
-        if kind is not None:
-            s.channel(kind, [w.channel[1]])
-        dt = time.perf_counter() - t0
-        terms_in = n0 + int(ctr[2][:-1].sum())
-        out.append((terms_in, dt))
-    if q is not None:
-        q.put(out)
-    return out
+def _oracle_worker(wname, n_warm, n_runs, barrier, q):
+    """Reference-arm worker: n_warm warm-up runs of the circuit's first two layers,
+    then (after all workers reach the barrier) n_runs whole-circuit runs."""
+    for _ in range(n_warm):
+        _oracle_whole_circuit(wname, layers=2)
+    barrier.wait()
+    q.put([_oracle_whole_circuit(wname) for _ in range(n_runs)])
 
 
-def cpu_baseline_from_snapshot(g_arrays, w, gens_layer):
-    """Single-thread oracle timing of one layer from a GPU snapshot (identical state)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import orc
-    import pauliprop as pp
-    z, x, c = g_arrays
-    f = tuple(pp.compile_filter(strategy_of(w)))
-    kind = {"depolarizing": 0, "dephasing": 1}[w.channel[0]] if w.channel else None
-    v = orc.OracleSPV(w.N, max(16, 2 * len(c)), max(16, 2 * len(c)))
-    v.upload(z, x, c)
-    n0 = len(v)
-    t0 = time.perf_counter()
-    _, ctr = v.evolve(gens_layer, w.angles, window=1, strict=f, nwin=len(gens_layer))
-    if kind is not None:
-        v.channel(kind, [w.channel[1]])
-    dt = time.perf_counter() - t0
-    return n0 + int(ctr[2][:-1].sum()), dt, v
+def _oracle_background(wname, out_path, q):
+    """One whole-circuit oracle run for the GPU arm's CPU baseline and final check."""
+    q.put(_oracle_whole_circuit(wname, out_path=out_path))
+
+
+def workload_label(w):
+    return (f"{w.name}: N={w.N}, {w.layers} layers x {len(w.layer)} rotations, "
+            f"thresh {w.thresh}, wmax {w.wmax}, channel {w.channel}")
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -262,36 +258,45 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned truncation "
                           "(its plain threshold path is the plain arm of this workload)"}), flush=True)
         return
-    reps = args.warmup + args.steps
-    procs = [ctx.Process(target=_oracle_layer_sample, args=(args.workload, SNAP_LAYER, reps, q))
-             for _ in range(nthreads)]
+    # the K timed whole-circuit runs are dealt round-robin to P single-threaded
+    # worker processes that run concurrently (the reference path is serial:
+    # spv_kernels.jl:3-5); the W warm-up steps are short runs of the first two layers
+    P = max(1, min(nthreads, args.steps))
+    runs = [args.steps // P + (1 if k < args.steps % P else 0) for k in range(P)]
+    warm = [args.warmup // P + (1 if k < args.warmup % P else 0) for k in range(P)]
+    barrier = ctx.Barrier(P)
+    procs = [ctx.Process(target=_oracle_worker, args=(args.workload, warm[k], runs[k], barrier, q))
+             for k in range(P)]
     for p in procs:
         p.start()
     res = [q.get() for _ in procs]
     for p in procs:
         p.join()
-    # per step: aggregate throughput of all workers (timed steps only)
-    per_step = []
-    for s in range(args.warmup, reps):
-        per_step.append(sum(r[s][0] / r[s][1] for r in res))
-    value = statistics.median(per_step)
-    w = workload(args.workload)
-    terms_in = res[0][args.warmup][0]
-    whole = w.layers <= SNAP_LAYER
-    what = (f"{w.name} end to end ({w.layers} layers x {len(w.layer)} rotations from the observable)" if whole
-            else f"{w.name} layer {SNAP_LAYER + 1} from the layer-{SNAP_LAYER} state")
+    # aggregate throughput of the concurrently running workers: the sum over
+    # workers of (term-rotations they processed / seconds they spent)
+    value = sum(sum(r["terms_in"] for r in rs) / sum(r["seconds"] for r in rs) for rs in res)
+    flat = [r for rs in res for r in rs]
+    per_run = statistics.median(r["terms_in"] / r["seconds"] for r in flat)
+    libs = sorted({lib for r in flat for lib in r["libs"]})
+    from pauliprop import circuits
+    w = {"lattice64": circuits.lattice64, "chain20": circuits.chain20,
+         "graph127": circuits.random_graph127}[args.workload]()
     line = {
         "metric": "terms/s rotate+merge+clip", "value": value, "unit": "terms/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * terms_in / (value / nthreads), "higher_is_better": True,
+        "ms_per_step": 1e3 * statistics.median(r["seconds"] for r in flat), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded circuit)", "impl": "reference",
-        "config": {"workload": what, "N": w.N,
-                   "rotations_per_sample": len(w.layer) * (w.layers if whole else 1), "threads": nthreads},
-        "cpu_baseline": {"value": value, "unit": "terms/s", "cores": nthreads, "kind": "port",
-                         "sample": (f"{what}, per worker process" if whole else
-                                    f"{w.name}: one Trotter layer ({len(w.layer)} rotations + channel) "
-                                    f"from the layer-{SNAP_LAYER} state, per worker process")},
+        "config": {"workload": workload_label(w), "N": w.N, "threads": P,
+                   "value_is": f"aggregate of {P} concurrent single-threaded runs (sum of per-worker terms/s)",
+                   "per_run_single_thread_terms_per_s": per_run,
+                   "runs_per_worker": runs, "step": "one whole-circuit run from the observable"},
+        "expectation": flat[0]["expect"],
+        "native_libs_loaded": libs,
+        "cpu_baseline": {"value": value, "unit": "terms/s", "cores": P, "kind": "port",
+                         "sample": f"{w.name} end to end ({w.layers} layers x {len(w.layer)} rotations + channels "
+                                   f"from the observable), {args.steps} runs over {P} concurrent worker processes, "
+                                   f"C restatement of the reference path (oracle/liborc.so)"},
         "e2e": {"value": value, "unit": "terms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -565,8 +570,18 @@ def run_learned_bench(args):
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args):
     import numpy as np
-    import torch
     ws, rank, local = dist_init("nccl")
+    # CPU baseline and final check: one whole-circuit oracle run in a spawned
+    # process, started before the first CUDA call, running while the GPU is timed
+    orc_proc = orc_q = orc_path = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        orc_q = ctx.Queue()
+        orc_path = tempfile.NamedTemporaryFile(suffix=".npz", delete=False).name
+        orc_proc = ctx.Process(target=_oracle_background, args=(args.workload, orc_path, orc_q))
+        orc_proc.start()
+    import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     import pauliprop as pp
@@ -637,6 +652,7 @@ def run_ours(args):
     hc = torch.from_numpy(obs_c.copy()).pin_memory()
     h2d = d2h = 0
     te = []
+    final = None
     for _ in range(args.steps):
         if ws > 1:
             torch.distributed.barrier()
@@ -654,6 +670,7 @@ def run_ours(args):
         te.append(time.perf_counter() - t0)
         h2d = obs_z.nbytes + obs_x.nbytes + obs_c.nbytes + len(gens) * (2 * 8 * nw + 16)
         d2h = zf.nbytes + xf.nbytes + cf.nbytes + 8
+        final = (zf, xf, cf, ev)
     t_e2e = reduce_max(sum(te), ws, dev)
     e2e_value = total_terms / t_e2e
 
@@ -665,48 +682,29 @@ def run_ours(args):
     pipe_bytes = B * (sp["terms_in"] + sp["merge_out"])          # B*(n + m) per rotation, summed
     hbm, src = peaks()
 
-    # CPU baseline on an identical snapshot (rank 0 at N=1)
+    # CPU baseline (the concurrent whole-circuit oracle run) and the final check
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and w.layers <= SNAP_LAYER:
-        # a circuit this short is timed end to end on the oracle, and the GPU's
-        # final term set is checked against the oracle's
-        ti_cpu, dt_cpu, vorc = _oracle_full_run(w)
-        upload_dev()
-        pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0)
-        gz_, gx_, gc_ = g.to_arrays()
-        oz_, ox_, oc_ = vorc.arrays()
-        same = bool(np.array_equal(gz_, oz_) and np.array_equal(gx_, ox_)
-                    and np.abs(gc_ - oc_).max(initial=0.0) <= 1e-12 * max(1.0, np.abs(oc_).max(initial=1.0)))
-        cpu = {"value": ti_cpu / dt_cpu, "unit": "terms/s", "cores": 1, "kind": "port",
-               "sample": f"{w.name} end to end ({w.layers} layers x {per} rotations from the observable), "
-                         f"C restatement of the reference path, 1 thread",
-               "gpu_matches_oracle_on_sample": same}
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and w.layers > SNAP_LAYER:
-        upload_dev()
-        pp.evolve_(g, w.layer * SNAP_LAYER, w.angles * SNAP_LAYER, truncation=strat, channel=ch,
-                   channel_every=per if ch else 0)
-        snap = g.to_arrays()
-        ti_cpu, dt_cpu, vorc = cpu_baseline_from_snapshot(snap, w, [(p.z, p.x) for p in w.layer])
-        # same sample on the GPU, and its result against the oracle's
-        g.upload(*snap, sorted=True)
-        torch.cuda.synchronize()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        st2 = {}
-        pp.evolve_(g, w.layer, w.angles, truncation=strat, channel=ch, stats=st2)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        gz_, gx_, gc_ = g.to_arrays()
-        oz_, ox_, oc_ = vorc.arrays()
-        same = bool(np.array_equal(gz_, oz_) and np.array_equal(gx_, ox_)
-                    and np.abs(gc_ - oc_).max(initial=0.0) <= 1e-12 * max(1.0, np.abs(oc_).max(initial=1.0)))
-        cpu = {"value": ti_cpu / dt_cpu, "unit": "terms/s", "cores": 1, "kind": "port",
-               "sample": f"{w.name} layer {SNAP_LAYER + 1} ({len(w.layer)} rotations + channel) from the "
-                         f"GPU's layer-{SNAP_LAYER} state ({len(snap[2])} terms), C restatement of the "
-                         f"reference path, 1 thread",
-               "gpu_same_sample_terms_per_s": st2["terms_in"] / (s0.elapsed_time(s1) * 1e-3),
-               "gpu_matches_oracle_on_sample": same}
+    final_check = None
+    if orc_proc is not None:
+        r = orc_q.get()
+        orc_proc.join()
+        o = np.load(orc_path)
+        os.unlink(orc_path)
+        zf, xf, cf, ev = final
+        keys_equal = bool(np.array_equal(zf, o["z"]) and np.array_equal(xf, o["x"]))
+        cdiff = float(np.abs(cf - o["c"]).max(initial=0.0)) if keys_equal else None
+        ctol = 1e-12 * max(1.0, float(np.abs(o["c"]).max(initial=1.0)))
+        diag = np.all(o["x"] == 0, axis=1)
+        etol = 1e-12 * max(1.0, float(np.abs(o["c"][diag]).sum()))
+        final_check = {"final_matches_oracle": bool(keys_equal and cdiff <= ctol and abs(ev - r["expect"]) <= etol),
+                       "keys_bit_exact": keys_equal, "max_coef_diff": cdiff, "coef_tol": ctol,
+                       "expectation_gpu": ev, "expectation_oracle": r["expect"], "expectation_tol": etol,
+                       "terms_final": int(len(cf))}
+        cpu = {"value": r["terms_in"] / r["seconds"], "unit": "terms/s", "cores": 1, "kind": "port",
+               "sample": f"{w.name} end to end ({w.layers} layers x {per} rotations + channels from the "
+                         f"observable, {r['terms_in']:.4g} term-rotations, {r['seconds']:.1f} s), C restatement "
+                         f"of the reference path (oracle/liborc.so), 1 thread, run while the GPU was timed",
+               "native_libs_loaded": r["libs"]}
 
     if rank == 0:
         line = {
@@ -714,12 +712,12 @@ def run_ours(args):
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded circuit)",
-            "config": {"workload": f"{w.name}: N={w.N}, {w.layers} layers x {per} rotations, "
-                                   f"thresh {w.thresh}, wmax {w.wmax}, channel {w.channel}",
+            "config": {"workload": workload_label(w),
                        "terms_in_per_step": terms_in, "peak_terms": st["peak"],
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "no flush: working set exceeds L2 at peak; the step re-creates its input"},
             "expectation": expect,
+            "final_check": final_check,
             "e2e": {"value": e2e_value, "unit": "terms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

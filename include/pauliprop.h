@@ -238,11 +238,12 @@ int pp_compact(pp_spv *h, const pp_filter *f);
  * z_out / x_out / c_out (device arrays with room for n terms), and stores their
  * count in *n_out (host).  Allocates nothing: its look-back scratch is a static
  * device array of 8 + PP_COMPACT_STATIC_MAX_TERMS/1024 words that every GPU loading
- * the library holds until exit.  The first call on a device looks up that array's
- * address, so make it before any stream capture.  All calls share the scratch:
- * calls whose work overlaps on the GPU race on it.  n > PP_COMPACT_STATIC_MAX_TERMS
- * gives PP_ARGUMENT_ERROR.  stream: a cudaStream_t (NULL: the default stream); the
- * call synchronizes it. */
+ * the library holds until exit.  The first call in each CUDA context on a device looks
+ * up that array's address, so make it before any stream capture.  All calls share
+ * the scratch: calls whose work overlaps on the GPU race on it.
+ * n > PP_COMPACT_STATIC_MAX_TERMS gives PP_ARGUMENT_ERROR.  stream: a cudaStream_t
+ * (NULL: the default stream); every call synchronizes it before returning, because
+ * the survivor count is read back to *n_out. */
 int pp_compact_static(int32_t N, const void *z, const void *x, const double *c, int64_t n, const pp_filter *f,
                       void *z_out, void *x_out, double *c_out, int64_t *n_out, void *stream);
 /* _apply!(v, ::AdaptiveTruncation) (spv_evolve.jl:103-114). */

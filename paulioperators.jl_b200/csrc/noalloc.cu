@@ -15,6 +15,7 @@
 // process exit.  All calls share it: each call clears the part it uses before
 // its kernel runs, and two calls whose work overlaps on the GPU (for example on
 // two streams) race on it and produce wrong results.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -156,25 +157,62 @@ __global__ void __launch_bounds__(NA_THREADS) k_compact_static(const u64 *Z, con
 using namespace pp;
 
 int pp_fail_msg(int code, const char *msg);   // sets pp_last_error() (api.cu)
-static std::mutex g_na_mu;
-static unsigned long long *g_na_ptr[64];   // device address of the scratch, per device
 
-// Device address of the scratch array on the current device.  Host code only
-// holds a stand-in for a __device__ symbol; the address must be queried once per
-// device, with that device current, before a kernel can be given it.
+// Device address of the scratch array in the calling thread's current CUDA
+// context.  Host code only holds a stand-in for a __device__ symbol; the address
+// must be looked up with the device current before a kernel can be given it.
+// The lookup is made once per context and cached under the context's unique id
+// (cuCtxGetId), so a context created after cudaDeviceReset, or another context on
+// the same device, gets its own lookup instead of a stale address.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+struct NaCache {
+    unsigned long long ctx_id;
+    unsigned long long *ptr;
+};
+static std::mutex g_na_mu;
+static NaCache g_na_cache[64];            // per device: the context id of the last lookup and its address
+static CtxGetCurrentFn g_ctx_current = nullptr;
+static CtxGetIdFn g_ctx_id = nullptr;
+
+static int na_context_id(unsigned long long *id) {
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 1;
+    return g_ctx_id(ctx, id) == CUDA_SUCCESS ? 0 : 1;
+}
+
 static int na_scratch(unsigned long long **out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
         return pp_fail_msg(PP_DEVICE_ERROR, "no usable CUDA device");
     std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_compact_scratch);
-        if (e != cudaSuccess)
-            return pp_fail_msg(PP_DEVICE_ERROR, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)).c_str());
-        g_na_ptr[dev] = (unsigned long long *)p;
+    if (!g_ctx_current || !g_ctx_id) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            return pp_fail_msg(PP_DEVICE_ERROR, "pp_compact_static: driver context queries unavailable");
+        g_ctx_current = (CtxGetCurrentFn)f1;
+        g_ctx_id = (CtxGetIdFn)f2;
     }
-    *out = g_na_ptr[dev];
+    unsigned long long id = 0;
+    const bool have_ctx = na_context_id(&id) == 0;
+    NaCache &c = g_na_cache[dev];
+    if (have_ctx && c.ptr && c.ctx_id == id) {
+        *out = c.ptr;
+        return PP_OK;
+    }
+    // first call in this context (the lookup also makes the runtime's context current)
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_compact_scratch);
+    if (e != cudaSuccess)
+        return pp_fail_msg(PP_DEVICE_ERROR, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)).c_str());
+    if (na_context_id(&id) != 0) return pp_fail_msg(PP_DEVICE_ERROR, "pp_compact_static: no current CUDA context");
+    c.ctx_id = id;
+    c.ptr = (unsigned long long *)p;
+    *out = c.ptr;
     return PP_OK;
 }
 

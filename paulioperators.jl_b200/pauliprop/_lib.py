@@ -11,6 +11,8 @@ import os
 from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_int64, c_uint8, c_uint64,
                     c_void_p)
 
+from .errors import ArgumentError, DeviceError, DimensionMismatch, PauliPropError
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PAULIPROP_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libpauliprop.so")
 
@@ -22,22 +24,6 @@ PP_OUT_OF_MEMORY = 4
 PP_DEVICE_ERROR = 5
 PP_TIMEOUT = 6
 PP_NOT_IMPLEMENTED = 7
-
-
-class ArgumentError(ValueError):
-    """Julia ArgumentError (bad probability, qubit index, window, strategy kind)."""
-
-
-class DimensionMismatch(ValueError):
-    """Julia DimensionMismatch (generators and angles of different length)."""
-
-
-class PauliPropError(RuntimeError):
-    """Julia ErrorException (N > 128, complex coefficient for real storage, broken invariant)."""
-
-
-class DeviceError(RuntimeError):
-    """CUDA runtime failure, or no CUDA device present."""
 
 
 class PPFilter(Structure):

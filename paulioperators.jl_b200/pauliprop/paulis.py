@@ -7,7 +7,7 @@ N <= 64, two (low, high) for N <= 128.
 """
 import numpy as np
 
-from ._lib import PauliPropError
+from .errors import PauliPropError
 
 INT64_MAX = 2**63 - 1
 
@@ -163,7 +163,7 @@ def unpack_keys(z, x):
 
 def qubit_mask(N, qubits):
     """_qubit_mask (channels.jl:14-28); raises ArgumentError for an index outside 1:N."""
-    from ._lib import ArgumentError
+    from .errors import ArgumentError
     if qubits is None:
         return (1 << N) - 1 if N > 0 else 0
     if isinstance(qubits, (int, np.integer)):

@@ -1,8 +1,8 @@
 """bench.py's reference arm on the host cores (no GPU): the JSON line the round's
 driver reads -- metric, unit and direction of our arm, impl = "reference", a
-cpu_baseline describing the run, and an e2e entry with no host-device bytes.  The
-20-qubit chain (config 1) is short enough to time whole, end to end, from the
-observable."""
+cpu_baseline describing the run, and an e2e entry with no host-device bytes.  Each
+step is one whole-circuit run from the observable, the same configuration the GPU
+arm times, and the workers map no product library (only the oracle)."""
 import json
 import os
 import subprocess
@@ -22,9 +22,11 @@ def test_reference_arm_line_chain20():
     assert line["metric"] == "terms/s rotate+merge+clip" and line["unit"] == "terms/s"
     assert line["higher_is_better"] is True and line["steps"] == 2 and line["warmup"] == 1
     assert line["value"] > 0
-    assert "end to end" in line["config"]["workload"]
-    assert line["config"]["rotations_per_sample"] == 8 * 39
+    assert line["config"]["workload"].startswith("chain20: N=20, 8 layers x 39 rotations")
+    assert line["config"]["step"] == "one whole-circuit run from the observable"
+    assert sum(line["config"]["runs_per_worker"]) == 2
+    assert line["native_libs_loaded"] == ["oracle/_build/liborc.so"]
     cb = line["cpu_baseline"]
-    assert cb["kind"] == "port" and cb["cores"] == 2 and cb["value"] == line["value"] and cb["sample"]
+    assert cb["kind"] == "port" and cb["cores"] == 2 and "end to end" in cb["sample"] and cb["value"] == line["value"] and cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "terms/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

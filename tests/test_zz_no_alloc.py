@@ -7,7 +7,10 @@ the library.  This test gives it device arrays allocated by the test itself and
 checks two calls in a row — the second reuses the scratch the first one left
 behind — against the handle-based pp_compact on the same terms: identical keys
 and bit-identical coefficients (the same per-term predicate decides; nothing is
-summed).  Collected last so that a failure here never hides the other tests.
+summed), and against the CPU oracle's _compact_spv! restatement.  The filters
+cover every criterion of should_drop: coefficient, weight, X weight, Majorana
+weight and both exponentially damped thresholds, for one- and two-word keys.
+Collected last so that a failure here never hides the other tests.
 """
 import ctypes
 import random
@@ -15,8 +18,9 @@ import random
 import numpy as np
 import pytest
 
+import orc
 import pauliprop as pp
-from helpers import rand_terms, strategy
+from helpers import filt, rand_terms, strategy
 from pauliprop import _lib
 
 pytestmark = pytest.mark.gpu
@@ -64,6 +68,37 @@ def test_static_clip_matches_handle_clip_twice(N, n):
         assert 0 < len(rc) < n
         assert np.array_equal(sz, rz) and np.array_equal(sx, rx)
         assert np.array_equal(scf.view(np.uint64), rc.view(np.uint64))
+
+
+def _oracle_clip(N, z, x, c, spec):
+    v = orc.OracleSPV(N, max(16, len(c)), 16)
+    v.upload(z, x, c)
+    v.compact(filt(spec))
+    return v.arrays()
+
+
+@pytest.mark.parametrize("N", [40, 128])
+def test_static_clip_every_criterion(N):
+    """Every should_drop criterion (spv_kernels.jl:64-79) through the static entry
+    point, two calls in a row per filter, against pp_compact and the oracle."""
+    rng = random.Random(1000 + N)
+    terms = rand_terms(rng, N, 50_000)
+    keys = sorted(terms)
+    z, x = pp.pack_keys(N, keys)
+    c = np.array([terms[k] for k in keys])
+    aw, axw = 1.5 / (0.75 * N), 2.0 / N         # typical weight 3N/4 and X weight N/2 of random strings
+    specs = [("majorana", N), ("xweight", N // 2), ("wdamped", aw, 0.05), ("xwdamped", axw, 0.05),
+             ("comp", [("coeff", 0.05), ("majorana", N + 8), ("wdamped", aw, 0.02)])]
+    for spec in specs:
+        rz, rx, rc = _reference_clip(N, z, x, c, spec)
+        oz, ox, oc = _oracle_clip(N, z, x, c, spec)
+        assert np.array_equal(rz, oz) and np.array_equal(rx, ox)
+        assert 0 < len(rc) < len(c), spec
+        for _ in range(2):
+            sz, sx, scf = _static_clip(N, z, x, c, spec)
+            assert np.array_equal(sz, oz) and np.array_equal(sx, ox), spec
+            assert np.array_equal(scf.view(np.uint64), oc.view(np.uint64)), spec
+            assert np.array_equal(scf.view(np.uint64), rc.view(np.uint64)), spec
 
 
 def test_static_clip_rejects_oversize():
