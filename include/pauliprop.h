@@ -296,6 +296,31 @@ int pp_power_table(double lambda, int32_t kmax, double *out);
 /* Message of the last failing call on this thread. */
 const char *pp_last_error(void);
 
+/* Launch configuration of the bucketed window-1 rotations (no counterpart in the
+ * reference; results do not depend on it).  (bucket_cap, items_per_thread) must be
+ * a compiled variant: (256, 2), (256, 4), (512, 2), (512, 4), (1024, 4) or
+ * (1024, 8); one CTA holds two buckets with 2 * bucket_cap / items_per_thread
+ * threads.  load_div (3..16): bucketing aims at a mean load of at most
+ * bucket_cap / load_div.  chunk (8..256): rotations launched between host checks.
+ * pauliprop's autotuner (pauliprop/tune.py) measures the variants on the device
+ * and caches the fastest per (word count, SM count); a new handle starts with
+ * (512, 4, 5, 64). */
+typedef struct {
+    int32_t bucket_cap, items_per_thread, load_div, chunk;
+} pp_tuning;
+int pp_set_tuning(pp_spv *h, const pp_tuning *t);
+int pp_get_tuning(pp_spv *h, pp_tuning *t);
+
+/* Test hooks for failure detection (no counterpart in the reference, which has no
+ * device).  pp_debug_fail_alloc: the after-th next device allocation of any handle
+ * fails with PP_OUT_OF_MEMORY, once (after <= 0 disarms); every growth is
+ * transactional, so the handle keeps its previous live set.
+ * pp_debug_lookback_timeout: runs one look-back wait on a status that nothing
+ * publishes, bounded by limit polls (1..2^22); returns PP_TIMEOUT when the wait
+ * gives up as it must, and the device stays usable. */
+int pp_debug_fail_alloc(int64_t after);
+int pp_debug_lookback_timeout(int64_t limit);
+
 #ifdef __cplusplus
 }
 #endif

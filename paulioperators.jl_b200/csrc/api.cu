@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,7 @@
 #include "kernels_stoch.cuh"
 #include "kernels_algebra.cuh"
 #include "kernels_small.cuh"
+#include "kernels_bucket.cuh"
 
 using namespace pp;
 
@@ -107,6 +109,22 @@ struct pp_spv {
     long long *hrange = nullptr, *hnout = nullptr;
     cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
     long long gexec_gen[3] = {-1, -1, -1};
+    // bucketed window-1 rotations (kernels_bucket.cuh): two bucket sets of
+    // 2^bk_bits_cap buckets of bk_cap slots, hash rows, per-rotation records,
+    // dense offsets, and the captured rotation graphs per bucket count
+    u64 *bkz[2] = {nullptr, nullptr}, *bkx[2] = {nullptr, nullptr};
+    double *bkc[2] = {nullptr, nullptr};
+    int *bkcnt[2] = {nullptr, nullptr};
+    int bk_bits_cap = -1;
+    int bk_cap = 0;
+    u64 *bk_rows = nullptr;
+    BkRec *bk_rec = nullptr;
+    long long bk_rec_cap = 0;
+    long long *bk_off = nullptr;
+    int *bk_aux = nullptr;                  // [0] largest scatter count, [1] scatter error bits
+    std::unordered_map<int, cudaGraphExec_t> bk_graphs;   // key: bits * 4 + chunk class
+    long long bk_graph_gen = -1;
+    pp_tuning tune = {BK_DEFAULT_CAP, BK_DEFAULT_ITEMS, 5, 64};   // pp_set_tuning
 };
 
 // ------------------------------------------------------------------ helpers
@@ -124,9 +142,14 @@ static void dfree(pp_spv *h, void *p) {
 // old one is freed, so a failure leaves *p (and everything sized from it) as it
 // was: callers update their capacity fields only after every allocation of a
 // growth step succeeded, and the handle stays usable after an out-of-memory.
+// Test hook (pp_debug_fail_alloc): the k-th next device allocation fails.
+static std::atomic<long long> g_fail_alloc_after{0};
+
 template <typename T>
 static int dalloc(pp_spv *h, T **p, long long count) {
     if (count <= 0) count = 1;
+    if (g_fail_alloc_after.load() > 0 && g_fail_alloc_after.fetch_sub(1) == 1)
+        return fail(PP_OUT_OF_MEMORY, "cudaMalloc: injected allocation failure (pp_debug_fail_alloc)");
     void *q = nullptr;
     const size_t b = (size_t)count * sizeof(T);
     cudaError_t e = cudaMalloc(&q, b);
@@ -174,23 +197,34 @@ static int write_state(pp_spv *h, const DevState *st) {
     return PP_OK;
 }
 
-// Merge/rotate workspaces sized from the live and append capacities.
-static int alloc_merge_ws(pp_spv *h) {
-    long long need = (h->cap + std::max(h->cap, h->acap_phys)) / B_D + 4;
+// Merge/rotate workspaces sized for live capacity cap and append capacity acap.
+// Every buffer of a growth is allocated before any is replaced, so a failure
+// leaves the workspaces (and the capacities they were sized for) as they were.
+static int alloc_merge_ws(pp_spv *h, long long cap, long long acap) {
+    const long long need = (cap + std::max(cap, acap)) / B_D + 4;
     if (need > h->nsplit_cap) {
-        TRY(dalloc(h, &h->split_i, need + 1));
-        TRY(dalloc(h, &h->split_j, need + 1));
-        TRY(dalloc(h, &h->split_k, need + 1));
-        TRY(dalloc(h, &h->kcnt, need + 1));
-        TRY(dalloc(h, &h->sphys, need + 1));
-        TRY(dalloc(h, &h->soff, need + 1));
-        TRY(dalloc(h, &h->tstat, need));
-        TRY(dalloc(h, &h->part, need * 4));
+        int *t[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        u64 *ts = nullptr;
+        double *tp = nullptr;
+        int r = 0;
+        for (int i = 0; i < 6 && !r; ++i) r = dalloc(h, &t[i], need + 1);
+        if (!r) r = dalloc(h, &ts, need);
+        if (!r) r = dalloc(h, &tp, need * 4);
+        if (r) {
+            for (int i = 0; i < 6; ++i) dfree(h, t[i]);
+            dfree(h, ts);
+            dfree(h, tp);
+            return r;
+        }
+        int **dst[6] = {&h->split_i, &h->split_j, &h->split_k, &h->kcnt, &h->sphys, &h->soff};
+        for (int i = 0; i < 6; ++i) { dfree(h, *dst[i]); *dst[i] = t[i]; }
+        dfree(h, h->tstat); h->tstat = ts;
+        dfree(h, h->part); h->part = tp;
         CU(cudaMemsetAsync(h->tstat, 0, need * sizeof(u64), h->stream));
         h->nsplit_cap = need;
     }
-    long long g = (h->cap + h->acap_phys) / G_TILE + 4;
-    if (h->acap_phys > 0 && g > h->gtiles_cap) {
+    const long long g = (cap + acap) / G_TILE + 4;
+    if (acap > 0 && g > h->gtiles_cap) {
         TRY(dalloc(h, &h->gstat, g));
         CU(cudaMemsetAsync(h->gstat, 0, g * sizeof(u64), h->stream));
         h->gtiles_cap = g;
@@ -218,7 +252,9 @@ static int ensure_dense(pp_spv *h) {
 
 // Allocates live sets and structured-path workspaces for capacity newcap,
 // preserving the live terms (copied into set 0).
-static int grow_live(pp_spv *h, long long need) {
+// With preserve == false the live terms are not copied (the caller refills the
+// sets) and the state's live count becomes 0 once the new sets are in place.
+static int grow_live(pp_spv *h, long long need, bool preserve = true) {
     long long newcap = std::max(need, std::max(2 * h->cap, (long long)4096));
     if (newcap > 0x7fffffffll - 8192) newcap = std::max(need, 0x7fffffffll - 8192);
     if (need > 0x7fffffffll - 8192) return fail(PP_OUT_OF_MEMORY, "term count exceeds 2^31 - 8192");
@@ -238,19 +274,36 @@ static int grow_live(pp_spv *h, long long need) {
                                                   " terms would leave less than 4 GiB of device memory free");
         }
     }
-    // both new term sets first; on failure the handle is unchanged
+    // every new buffer first; on failure the handle is unchanged
     u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
     double *nc[2] = {nullptr, nullptr};
+    int *nsrcidx = nullptr, *nsrc = nullptr, *noffA = nullptr, *nhfirst = nullptr, *nfwd = nullptr, *nbwd = nullptr;
+    unsigned *nmeta = nullptr;
+    TileAggA *nagg = nullptr;
     auto drop = [&]() {
         for (int s = 0; s < 2; ++s) { dfree(h, nz[s]); dfree(h, nx[s]); dfree(h, nc[s]); }
+        dfree(h, nsrcidx); dfree(h, nsrc); dfree(h, noffA); dfree(h, nhfirst); dfree(h, nfwd); dfree(h, nbwd);
+        dfree(h, nmeta); dfree(h, nagg);
     };
-    for (int s = 0; s < 2; ++s) {
-        int r = dalloc(h, &nz[s], newcap * h->NW);
+    const long long ta = newcap / SEG + 4;
+    int r = 0;
+    for (int s = 0; s < 2 && !r; ++s) {
+        r = dalloc(h, &nz[s], newcap * h->NW);
         if (!r) r = dalloc(h, &nx[s], newcap * h->NW);
         if (!r) r = dalloc(h, &nc[s], newcap);
-        if (r) { drop(); return r; }
     }
+    if (!r) r = dalloc(h, &nsrcidx, newcap + SEG);
+    if (!r) r = dalloc(h, &nmeta, newcap + SEG);
+    if (!r) r = dalloc(h, &nsrc, newcap + SEG);
+    if (!r) r = dalloc(h, &nagg, ta);
+    if (!r) r = dalloc(h, &noffA, ta);
+    if (!r) r = dalloc(h, &nhfirst, ta);
+    if (!r) r = dalloc(h, &nfwd, ta * TAU_MAX);
+    if (!r) r = dalloc(h, &nbwd, ta * TAU_MAX);
+    if (!r) r = alloc_merge_ws(h, newcap, h->acap_phys);   // transactional itself; larger workspaces are harmless
+    if (r) { drop(); return r; }
     cudaError_t ce = cudaSuccess;
+    if (have && !preserve) st.n = 0;
     if (have && st.n > 0) {
         ce = cudaMemcpyAsync(nz[0], h->z[st.cur], st.n * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream);
         if (ce == cudaSuccess)
@@ -263,28 +316,26 @@ static int grow_live(pp_spv *h, long long need) {
         dfree(h, h->z[s]); dfree(h, h->x[s]); dfree(h, h->c[s]);
         h->z[s] = nz[s]; h->x[s] = nx[s]; h->c[s] = nc[s];
     }
+    dfree(h, h->srcidx); h->srcidx = nsrcidx;
+    dfree(h, h->meta); h->meta = nmeta;
+    dfree(h, h->src); h->src = nsrc;
+    dfree(h, h->aggA); h->aggA = nagg;
+    dfree(h, h->offA); h->offA = noffA;
+    dfree(h, h->hfirstA); h->hfirstA = nhfirst;
+    dfree(h, h->fwdA); h->fwdA = nfwd;
+    dfree(h, h->bwdA); h->bwdA = nbwd;
+    h->cap = newcap;
     if (have) {
-        // the live terms are in set 0 from here on, whatever fails below
+        // the live terms (if kept) are in set 0 from here on
         st.cur = 0;
         TRY(write_state(h, &st));
     }
-    TRY(dalloc(h, &h->srcidx, newcap + SEG));
-    TRY(dalloc(h, &h->meta, newcap + SEG));
-    TRY(dalloc(h, &h->src, newcap + SEG));
-    long long ta = newcap / SEG + 4;
-    TRY(dalloc(h, &h->aggA, ta));
-    TRY(dalloc(h, &h->offA, ta));
-    TRY(dalloc(h, &h->hfirstA, ta));
-    TRY(dalloc(h, &h->fwdA, ta * TAU_MAX));
-    TRY(dalloc(h, &h->bwdA, ta * TAU_MAX));
-    h->cap = newcap;
-    TRY(alloc_merge_ws(h));
     return PP_OK;
 }
 
-static int ensure_live(pp_spv *h, long long need) {
+static int ensure_live(pp_spv *h, long long need, bool preserve = true) {
     if (need <= h->cap) return PP_OK;
-    return grow_live(h, need);
+    return grow_live(h, need, preserve);
 }
 
 // General path: physical append buffers (keeping pending appends) and sort temps.
@@ -296,6 +347,7 @@ static int ensure_append(pp_spv *h, long long need, long long pending) {
         int r = dalloc(h, &nz, nc * h->NW);
         if (!r) r = dalloc(h, &nx, nc * h->NW);
         if (!r) r = dalloc(h, &ncc, nc);
+        if (!r) r = alloc_merge_ws(h, h->cap, nc);
         if (r) { dfree(h, nz); dfree(h, nx); dfree(h, ncc); return r; }
         if (pending > 0) {
             CU(cudaMemcpyAsync(nz, h->az, pending * h->NW * 8, cudaMemcpyDeviceToDevice, h->stream));
@@ -306,7 +358,6 @@ static int ensure_append(pp_spv *h, long long need, long long pending) {
         dfree(h, h->az); dfree(h, h->ax); dfree(h, h->ac);
         h->az = nz; h->ax = nx; h->ac = ncc;
         h->acap_phys = nc;
-        TRY(alloc_merge_ws(h));
     }
     if (std::max(h->acap_phys, h->cap) > h->tcap) {
         long long tc = std::max(h->acap_phys, h->cap);
@@ -522,6 +573,15 @@ static void launch_merge(pp_spv *h, const Bufs &B, int flags) {
     k_commit<MODE><<<1, 256, 0, s>>>(B, flags);
 }
 
+// Digit-histogram and scan workspaces of a radix sort of n records.
+static int radix_reserve(pp_spv *h, long long n) {
+    const long long m = 256ll * ((n + R_TILE - 1) / R_TILE);
+    if (m > h->rhist_cap) { TRY(dalloc(h, &h->rhist, m)); h->rhist_cap = m; }
+    const long long nb = (m + SC_TILE - 1) / SC_TILE;
+    if (nb > h->rsums_cap) { TRY(dalloc(h, &h->rsums, nb)); h->rsums_cap = nb; }
+    return PP_OK;
+}
+
 // Stable LSD radix sort of n records in set A (za, xa, ca) using set T as the
 // ping-pong partner.  *in_t = 1 if the result ended in T.
 template <int NW>
@@ -537,9 +597,8 @@ static int radix_sort(pp_spv *h, u64 *za, u64 *xa, double *ca, u64 *zt, u64 *xt,
     CU(cudaStreamSynchronize(s));
     const int ntiles = (int)((n + R_TILE - 1) / R_TILE);
     const long long m = 256ll * ntiles;
-    if (m > h->rhist_cap) { TRY(dalloc(h, &h->rhist, m)); h->rhist_cap = m; }
+    TRY(radix_reserve(h, n));
     const long long nb = (m + SC_TILE - 1) / SC_TILE;
-    if (nb > h->rsums_cap) { TRY(dalloc(h, &h->rsums, nb)); h->rsums_cap = nb; }
     u64 *cz = za, *cx = xa, *oz = zt, *ox = xt;
     double *cc = ca, *oc = ct;
     int passes = 0;
@@ -617,6 +676,10 @@ extern "C" int pp_destroy(pp_spv *h) {
                     h->bcos, h->bsin, h->bend, h->hfin, h->hpart, h->heout, h->hrange, h->hnout, h->sel64, h->vtmp};
     for (void *p : ptrs) if (p) cudaFree(p);
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
+    for (auto &kv : h->bk_graphs) cudaGraphExecDestroy(kv.second);
+    void *bptrs[] = {h->bkz[0], h->bkz[1], h->bkx[0], h->bkx[1], h->bkc[0], h->bkc[1], h->bkcnt[0], h->bkcnt[1],
+                     h->bk_rows, h->bk_rec, h->bk_off, h->bk_aux};
+    for (void *p : bptrs) if (p) cudaFree(p);
     if (h->Ph) cudaFreeHost(h->Ph);
     if (h->gens_h) cudaFreeHost(h->gens_h);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -738,6 +801,389 @@ struct RunProf {
     long long launches = 0;
 };
 
+// ------------------------------------------------------------------ bucketed window-1 rotations
+// Window-1 rotations of a live set larger than k_small_run's shared memory run
+// one k_bk_rotate launch each over a hash-bucketed copy of the live set
+// (kernels_bucket.cuh); the sequence ends with a gather into a dense array and a
+// radix sort, so the live set is dense and sorted between calls as before.
+static int expect_dev(pp_spv *h, const u64 *k, double *out);
+static constexpr int BK_MIN_ROT = 32;     // shorter sequences keep the sorted-merge kernels
+
+// PAULIPROP_WINDOW1_PATH=tiles selects the sorted-merge kernels instead (both
+// give the same result; the switch exists for comparisons).
+static bool bk_enabled() {
+    const char *e = getenv("PAULIPROP_WINDOW1_PATH");
+    return e && strcmp(e, "buckets") == 0;
+}
+
+// Compiled variants of k_bk_rotate: (bucket capacity, items per thread).
+typedef void (*BkKernel)(BkArgs, int);
+struct BkVariant {
+    int cap, items, threads;
+    BkKernel k1, k2;
+    size_t smem1, smem2;
+};
+#define PP_BK_VARIANT(C, I)                                                                              \
+    { C, I, bk_threads<C, I>(), k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, bk_smem_bytes<1, C>(),       \
+      bk_smem_bytes<2, C>() }
+static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(256, 2), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(512, 2),
+                                        PP_BK_VARIANT(512, 4), PP_BK_VARIANT(1024, 4), PP_BK_VARIANT(1024, 8)};
+#undef PP_BK_VARIANT
+
+static const BkVariant *bk_variant(int cap, int items) {
+    for (const BkVariant &v : BK_VARIANTS)
+        if (v.cap == cap && v.items == items) return &v;
+    return nullptr;
+}
+
+template <int NW>
+static void bk_launch(pp_spv *h, const BkVariant *v, int bits, const BkArgs &A, int k) {
+    (NW == 1 ? v->k1 : v->k2)<<<1 << (bits - 1), v->threads, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
+}
+
+// Hash rows: fixed pseudo-random words (splitmix64 from a fixed seed), so the
+// bucket of a key never depends on the call.
+static int bk_rows_init(pp_spv *h) {
+    if (h->bk_rows) return PP_OK;
+    u64 rows[BK_ROWS * 4];
+    unsigned long long s = 0x5EEDB0C4E7ull;
+    for (int i = 0; i < BK_ROWS * 4; ++i) {
+        s += 0x9E3779B97F4A7C15ull;
+        unsigned long long z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        rows[i] = z ^ (z >> 31);
+    }
+    u64 *dr = nullptr;
+    int *da = nullptr;
+    TRY(dalloc(h, &dr, BK_ROWS * 4));
+    int r = dalloc(h, &da, 2);
+    if (r) { dfree(h, dr); return r; }
+    h->bk_rows = dr;
+    h->bk_aux = da;
+    CU(cudaMemcpyAsync(h->bk_rows, rows, sizeof rows, cudaMemcpyHostToDevice, h->stream));
+    for (const BkVariant &v : BK_VARIANTS) {
+        CU(cudaFuncSetAttribute(v.k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem1));
+        CU(cudaFuncSetAttribute(v.k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem2));
+    }
+    return sync_check(h);
+}
+
+// Smallest bucket count for n terms at a mean load of at most cap / load_div.
+static int bk_bits_for(long long n, int cap, int load_div) {
+    int b = 1;
+    while (b < BK_ROWS && ((long long)cap << b) < (long long)load_div * n) ++b;
+    return b;
+}
+
+static BkArgs bk_args(pp_spv *h, int bits, BkRec *rec) {
+    BkArgs A;
+    memset(&A, 0, sizeof A);
+    for (int s = 0; s < 2; ++s) { A.z[s] = h->bkz[s]; A.x[s] = h->bkx[s]; A.c[s] = h->bkc[s]; A.cnt[s] = h->bkcnt[s]; }
+    A.bits = bits;
+    A.rows = h->bk_rows;
+    A.rec = rec;
+    A.S = h->S;
+    A.P = h->P;
+    A.gens = h->gens;
+    return A;
+}
+
+// Scatters (SZ, SX, SC) -- dense n terms, or the bucket set `from` of 2^sbits
+// buckets -- into bucket set `to` with 2^bits buckets.  Returns the largest
+// bucket count in *maxcnt, or -1 if a bucket overflowed.
+template <int NW>
+static int bk_scatter(pp_spv *h, const u64 *SZ, const u64 *SX, const double *SC, long long n, int from, int sbits,
+                      int to, int bits, int *maxcnt) {
+    cudaStream_t s = h->stream;
+    const int cap = h->bk_cap;
+    CU(cudaMemsetAsync(h->bkcnt[to], 0, sizeof(int) << bits, s));
+    CU(cudaMemsetAsync(h->bk_aux, 0, 2 * sizeof(int), s));
+    const long long slots = from >= 0 ? ((long long)cap << sbits) : n;
+    const int grid = (int)std::max(1ll, std::min((slots + 255) / 256, (long long)h->nsm * 16));
+    k_bk_scatter<NW><<<grid, 256, 0, s>>>(SZ, SX, SC, n, from >= 0 ? h->bkcnt[from] : nullptr, sbits, h->bkz[to],
+                                          h->bkx[to], h->bkc[to], h->bkcnt[to], bits, cap, h->bk_rows, h->bk_aux,
+                                          h->bk_aux + 1);
+    int aux[2] = {0, 0};
+    CU(cudaMemcpyAsync(aux, h->bk_aux, sizeof aux, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    *maxcnt = (aux[1] & ERR_OVERFLOW) ? -1 : aux[0];
+    return PP_OK;
+}
+
+// Bucket sets for 2^bits buckets of the tuned capacity.  Growing the allocation
+// moves the live bucket set `*cur` (of 2^cur_bits buckets; cur_bits < 0: none)
+// into the new set 0.  Every buffer is allocated before the old ones are freed.
+template <int NW>
+static int bk_reserve(pp_spv *h, int bits, int *cur, int cur_bits) {
+    if (bits <= h->bk_bits_cap && h->bk_cap == h->tune.bucket_cap) return PP_OK;
+    if (cur_bits >= 0 && h->bk_cap != h->tune.bucket_cap)
+        return fail(PP_ERROR_EXCEPTION, "internal error: bucket capacity changed inside a call");
+    const int cap = h->tune.bucket_cap;
+    const int nbits = std::min(BK_ROWS, std::max(bits + 1, h->bk_cap == cap ? h->bk_bits_cap : 0));
+    const long long slots = (long long)cap << nbits;
+    {
+        size_t freeb = 0, totalb = 0;
+        if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) {
+            const double want = 2.0 * (double)slots * (16.0 * NW + 8.0);
+            if (want + 4.0 * (1ull << 30) > (double)freeb)
+                return fail(PP_OUT_OF_MEMORY, "bucketing " + std::to_string(slots) +
+                                                  " term slots would leave less than 4 GiB of device memory free");
+        }
+    }
+    u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
+    double *nc[2] = {nullptr, nullptr};
+    int *nn[2] = {nullptr, nullptr};
+    long long *noff = nullptr;
+    auto drop = [&]() {
+        for (int q = 0; q < 2; ++q) { dfree(h, nz[q]); dfree(h, nx[q]); dfree(h, nc[q]); dfree(h, nn[q]); }
+        dfree(h, noff);
+    };
+    int r = 0;
+    for (int q = 0; q < 2 && !r; ++q) {
+        r = dalloc(h, &nz[q], slots * NW);
+        if (!r) r = dalloc(h, &nx[q], slots * NW);
+        if (!r) r = dalloc(h, &nc[q], slots);
+        if (!r) r = dalloc(h, &nn[q], 1ll << nbits);
+    }
+    if (!r) r = dalloc(h, &noff, (1ll << nbits) + 1);
+    if (r) { drop(); return r; }
+    if (cur_bits >= 0 && h->bk_bits_cap >= 0) {
+        // the live bucket set keeps its layout: copy it into new set 0
+        const long long os = (long long)h->bk_cap << cur_bits;
+        cudaStream_t s = h->stream;
+        cudaError_t e = cudaMemcpyAsync(nz[0], h->bkz[*cur], os * NW * 8, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(nx[0], h->bkx[*cur], os * NW * 8, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(nc[0], h->bkc[*cur], os * 8, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(nn[0], h->bkcnt[*cur], sizeof(int) << cur_bits, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { drop(); return fail(PP_DEVICE_ERROR, cudaGetErrorString(e)); }
+        *cur = 0;
+    }
+    for (int q = 0; q < 2; ++q) {
+        dfree(h, h->bkz[q]); dfree(h, h->bkx[q]); dfree(h, h->bkc[q]); dfree(h, h->bkcnt[q]);
+        h->bkz[q] = nz[q]; h->bkx[q] = nx[q]; h->bkc[q] = nc[q]; h->bkcnt[q] = nn[q];
+    }
+    dfree(h, h->bk_off);
+    h->bk_off = noff;
+    h->bk_bits_cap = nbits;
+    h->bk_cap = cap;
+    return PP_OK;
+}
+
+// Moves the live bucket set *cur (2^*bits buckets) to a layout with more
+// buckets, doubling until the largest bucket holds at most half its capacity
+// (then no bucket of the next rotation's output can overflow).
+template <int NW>
+static int bk_regrid(pp_spv *h, int *cur, int *bits) {
+    int nbits = *bits;
+    for (;;) {
+        if (nbits + 1 > BK_ROWS) return fail(PP_OUT_OF_MEMORY, "bucketed live set exceeds 2^26 buckets");
+        ++nbits;
+        TRY(bk_reserve<NW>(h, nbits, cur, *bits));
+        int mx = 0;
+        TRY(bk_scatter<NW>(h, h->bkz[*cur], h->bkx[*cur], h->bkc[*cur], 0, *cur, *bits, *cur ^ 1, nbits, &mx));
+        if (mx >= 0 && mx <= h->bk_cap / 2) break;
+    }
+    *cur ^= 1;
+    *bits = nbits;
+    return PP_OK;
+}
+
+// Graph of `len` consecutive k_bk_rotate launches over 2^bits buckets.
+template <int NW>
+static int bk_graph(pp_spv *h, const BkVariant *v, int bits, int cls, int len, cudaGraphExec_t *out) {
+    if (h->bk_graph_gen != h->buf_gen) {
+        for (auto &kv : h->bk_graphs) cudaGraphExecDestroy(kv.second);
+        h->bk_graphs.clear();
+        h->bk_graph_gen = h->buf_gen;
+    }
+    const int key = bits * 4 + cls;
+    auto it = h->bk_graphs.find(key);
+    if (it != h->bk_graphs.end()) { *out = it->second; return PP_OK; }
+    const BkArgs A = bk_args(h, bits, h->bk_rec);
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < len; ++k) bk_launch<NW>(h, v, bits, A, k);
+    CU(cudaStreamEndCapture(h->stream, &graph));
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(PP_DEVICE_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    h->bk_graphs[key] = ex;
+    *out = ex;
+    return PP_OK;
+}
+
+// Gathers the bucket set `cur` (2^bits buckets) into live set 0 and
+// radix-sorts it: the live set is dense and sorted again.  Every allocation
+// comes first, so a failure leaves the dense live set as it was.
+template <int NW>
+static int bk_to_dense(pp_spv *h, int cur, int bits) {
+    const int nb = 1 << bits;
+    cudaStream_t s = h->stream;
+    k_bk_offsets<<<1, BKS_THREADS, 0, s>>>(h->bkcnt[cur], nb, h->bk_cap, h->bk_off);
+    long long n = 0;
+    CU(cudaMemcpyAsync(&n, h->bk_off + nb, sizeof n, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    TRY(radix_reserve(h, n));
+    TRY(ensure_live(h, n + 1, false));
+    k_bk_gather<NW><<<std::max(1, std::min(h->nsm * 8, (nb + 7) / 8)), 256, 0, s>>>(
+        h->bkz[cur], h->bkx[cur], h->bkc[cur], h->bkcnt[cur], nb, h->bk_cap, h->bk_off, h->z[0], h->x[0], h->c[0]);
+    TRY(sync_check(h));
+    int in_t = 0;
+    TRY(radix_sort<NW>(h, h->z[0], h->x[0], h->c[0], h->z[1], h->x[1], h->c[1], n, &in_t));
+    DevState st;
+    TRY(read_state(h, &st));
+    st.n = n;
+    st.cur = in_t;
+    st.seg_dense = 1;
+    TRY(write_state(h, &st));
+    return PP_OK;
+}
+
+// The window-1 sequence [start, L) on buckets.  The device cursor is at start.
+template <int NW>
+static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof, bool timed) {
+    TRY(ensure_dense(h));
+    TRY(bk_rows_init(h));
+    const BkVariant *var = bk_variant(h->tune.bucket_cap, h->tune.items_per_thread);
+    if (!var) return fail(PP_ERROR_EXCEPTION, "internal error: no compiled bucket variant for the tuning");
+    DevState st;
+    TRY(read_state(h, &st));
+    const long long n0 = st.n;
+    // per-rotation records rec[start .. L]
+    if (L + 1 > h->bk_rec_cap) {
+        TRY(dalloc(h, &h->bk_rec, L + 1));
+        h->bk_rec_cap = L + 1;
+    }
+    {
+        BkRec r0;
+        memset(&r0, 0, sizeof r0);
+        r0.n_in = n0;
+        r0.n_out = (unsigned long long)n0;
+        r0.acap = st.acap_logical;
+        CU(cudaMemcpyAsync(h->bk_rec + start, &r0, sizeof r0, cudaMemcpyHostToDevice, h->stream));
+        CU(cudaMemsetAsync(h->bk_rec + start + 1, 0, (L - start) * sizeof(BkRec), h->stream));
+    }
+    // bucket the live set
+    int bits = bk_bits_for(n0, h->tune.bucket_cap, h->tune.load_div), cur = 0;
+    for (;;) {
+        TRY(bk_reserve<NW>(h, bits, &cur, -1));
+        int mx = 0;
+        TRY(bk_scatter<NW>(h, h->z[st.cur], h->x[st.cur], h->c[st.cur], n0, -1, 0, 0, bits, &mx));
+        if (mx >= 0 && mx <= h->bk_cap / 2) break;
+        if (++bits > BK_ROWS) return fail(PP_OUT_OF_MEMORY, "bucketed live set exceeds 2^26 buckets");
+    }
+    cur = 0;
+    long long done = start;
+    cudaStream_t s = h->stream;
+    const int chunk = h->tune.chunk;
+    while (done < L) {
+        const long long len = std::min((long long)chunk, L - done);
+        k_bk_begin<<<1, 1, 0, s>>>(h->S, done, cur, 1);
+        prof->launches += 1;
+        if (!timed) {
+            long long r = 0;
+            while (r < len) {
+                const int cls = (len - r >= chunk) ? 0 : (len - r >= 8) ? 1 : 2;
+                const int cl = cls == 0 ? chunk : cls == 1 ? 8 : 1;
+                if (r > 0) {
+                    // a later graph of the chunk starts at rotation done + r
+                    k_bk_begin<<<1, 1, 0, s>>>(h->S, done + r, (cur + (int)r) & 1, 0);
+                    prof->launches += 1;
+                }
+                cudaGraphExec_t ex = nullptr;
+                TRY(bk_graph<NW>(h, var, bits, cls, cl, &ex));
+                CU(cudaGraphLaunch(ex, s));
+                prof->launches += cl;
+                r += cl;
+            }
+        } else {
+            const BkArgs A = bk_args(h, bits, h->bk_rec);
+            for (long long k = 0; k < len; ++k) {
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, s);
+                bk_launch<NW>(h, var, bits, A, (int)k);
+                cudaEventRecord(e1, s);
+                TRY(sync_check(h));
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                const long long r = done + k;
+                prof->t_merge += ms * 1e-3;
+                prof->launches += 1;
+                if (ctr && r < ctr->nwin && ctr->t_merge) ctr->t_merge[r] += ms * 1e-3;
+            }
+        }
+        TRY(sync_check(h));
+        TRY(read_state(h, &st));
+        if (st.err & ~ERR_OVERFLOW) return check_err(h, st);   // the dense live set is the sequence's input
+        const long long completed = (st.err & ERR_OVERFLOW) ? std::max(0ll, std::min(len, st.bk_fail - done)) : len;
+        cur = (cur + (int)(completed & 1)) & 1;
+        done += completed;
+        BkRec last;
+        CU(cudaMemcpyAsync(&last, h->bk_rec + done, sizeof last, cudaMemcpyDeviceToHost, s));
+        TRY(sync_check(h));
+        const bool over = (st.err & ERR_OVERFLOW) != 0;
+        if (over) {
+            st.err &= ~ERR_OVERFLOW;
+            TRY(write_state(h, &st));
+            CU(cudaMemsetAsync(h->bk_rec + done + 1, 0, sizeof(BkRec), s));
+        }
+        if (done < L && (over || last.maxcnt > h->bk_cap / 2)) TRY(bk_regrid<NW>(h, &cur, &bits));
+    }
+    // totals and counters of rotations [start, L)
+    std::vector<BkRec> rec((size_t)(L - start + 1));
+    CU(cudaMemcpyAsync(rec.data(), h->bk_rec + start, rec.size() * sizeof(BkRec), cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    TRY(read_state(h, &st));
+    std::vector<long long> rr;
+    if (h->rec_on) rr.assign((size_t)(4 * (L - start)), 0);
+    for (long long r = start; r < L; ++r) {
+        const BkRec &o = rec[(size_t)(r - start + 1)];
+        const long long n = o.n_in, a = (long long)o.created, tot = (long long)o.n_out, np = (long long)o.np;
+        st.live_in += n;
+        st.created += a;
+        st.merge_in += n + a;
+        st.merge_out += tot;
+        if (tot > st.peak) st.peak = tot;
+        if (o.pref) st.early += 1;
+        if (h->rec_on) {
+            // WindowCounters of the rotation (window = 1): an early boundary merges
+            // n -> np first, the regular one np + a -> total
+            long long *q = &rr[(size_t)(4 * (r - start))];
+            q[0] = a;
+            q[1] = (o.pref ? n + np : n) + a;
+            q[2] = (o.pref ? np : 0) + tot;
+            q[3] = o.pref ? 1 : 0;
+        }
+    }
+    if (h->rec_on && L > start)
+        CU(cudaMemcpy(h->rec + 4 * start, rr.data(), rr.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    {
+        // the early-merge capacity rule after the last rotation (as k_bk_rotate applies it)
+        const BkRec &o = rec.back();
+        long long acap = o.acap;
+        if (o.pref && (long long)o.np > acap) acap = std::max(2 * acap, (long long)o.np);
+        st.acap_logical = acap;
+    }
+    st.rot = L;
+    TRY(write_state(h, &st));
+    TRY(bk_to_dense<NW>(h, cur, bits));
+    // <ket|O|ket> after the last rotation (GEN_MEASURE), on the sorted live set
+    double ev = 0.0;
+    TRY(expect_dev(h, h->Ph->ket, &ev));
+    TRY(read_state(h, &st));
+    st.expect_val = ev;
+    st.measure_valid = 1;
+    TRY(write_state(h, &st));
+    return PP_OK;
+}
+
 // Structured window-1 sequence over rotations [start, L) (the device cursor
 // S->rot is at start): chunks of CHUNK_ROT rotations between state read-backs; on
 // ERR_OVERFLOW grow and resume at the rotation that stopped.  While the live set
@@ -751,6 +1197,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
     std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
     bool table = false;            // the device segment table describes the (dense) live set
     const bool small_ok = !timed && !h->batch_on && !h->Ph->local_active && h->Ph->corr_kind == 0;
+    const bool use_bk = bk_enabled() && !h->batch_on && h->Ph->corr_kind == 0;
     long long ncur = small_cap<NW>() + 1;   // live terms at the chunk's start (read when small_ok)
     if (small_ok) {
         DevState st;
@@ -772,6 +1219,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
             done = st.rot;
             continue;
         }
+        if (use_bk && L - done >= BK_MIN_ROT) return run_bucket<NW>(h, done, L, ctr, prof, timed);
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
@@ -1165,7 +1613,7 @@ static int run_general(pp_spv *h, const std::vector<GenRec> &G, long long window
             }
         }
         TRY(ensure_append(h, std::max(st.acap_logical, 2 * st.an + st.n), st.an));
-        TRY(alloc_merge_ws(h));
+        TRY(alloc_merge_ws(h, h->cap, h->acap_phys));
         Bufs B = make_bufs(h);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ctr && ctr->t_rotate) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, h->stream); }
@@ -1462,6 +1910,59 @@ extern "C" int pp_debug_phase_cycles(unsigned long long *out, int reset) {
     return PP_OK;
 }
 #endif
+
+// ------------------------------------------------------------------ tuning
+extern "C" int pp_set_tuning(pp_spv *h, const pp_tuning *t) {
+    if (!h || !t) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: null argument");
+    if (!bk_variant(t->bucket_cap, t->items_per_thread))
+        return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: (bucket_cap, items_per_thread) must be one of (256, 2), "
+                                       "(256, 4), (512, 2), (512, 4), (1024, 4), (1024, 8)");
+    if (t->load_div < 3 || t->load_div > 16) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: load_div must be in 3..16");
+    if (t->chunk < 8 || t->chunk > 256) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: chunk must be in 8..256");
+    if (t->bucket_cap != h->tune.bucket_cap || t->items_per_thread != h->tune.items_per_thread ||
+        t->chunk != h->tune.chunk) {
+        for (auto &kv : h->bk_graphs) cudaGraphExecDestroy(kv.second);
+        h->bk_graphs.clear();
+    }
+    h->tune = *t;
+    return PP_OK;
+}
+
+extern "C" int pp_get_tuning(pp_spv *h, pp_tuning *t) {
+    if (!h || !t) return fail(PP_ARGUMENT_ERROR, "pp_get_tuning: null argument");
+    *t = h->tune;
+    return PP_OK;
+}
+
+// ------------------------------------------------------------------ test hooks
+extern "C" int pp_debug_fail_alloc(int64_t after) {
+    g_fail_alloc_after.store(after > 0 ? after : 0);
+    return PP_OK;
+}
+
+// A look-back status that nothing publishes: tile 1's bounded wait on tile 0
+// must give up after `limit` polls and report ERR_TIMEOUT.
+static __device__ u64 g_dbg_status[2];
+static __device__ int g_dbg_err;
+
+__global__ void k_debug_lookback(long long limit) {
+    lookback_warp(g_dbg_status, 1, 1u, 7u, &g_dbg_err, limit);
+}
+
+extern "C" int pp_debug_lookback_timeout(int64_t limit) {
+    if (limit < 1 || limit > SPIN_LIMIT) return fail(PP_ARGUMENT_ERROR, "limit must be in 1..2^22");
+    const u64 zs[2] = {0, 0};
+    const int ze = 0;
+    CU(cudaMemcpyToSymbol(g_dbg_status, zs, sizeof zs));
+    CU(cudaMemcpyToSymbol(g_dbg_err, &ze, sizeof ze));
+    k_debug_lookback<<<1, 32>>>((long long)limit);
+    CU(cudaGetLastError());
+    CU(cudaDeviceSynchronize());
+    int e = 0;
+    CU(cudaMemcpyFromSymbol(&e, g_dbg_err, sizeof e));
+    if (e & ERR_TIMEOUT) return fail(PP_TIMEOUT, "a device-side look-back wait timed out (test hook: nothing publishes)");
+    return fail(PP_ERROR_EXCEPTION, "the look-back wait did not report its timeout");
+}
 
 extern "C" int pp_device_bytes(pp_spv *h, int64_t *bytes) {
     if (!h || !bytes) return fail(PP_ARGUMENT_ERROR, "null argument");

@@ -182,7 +182,8 @@ __device__ __forceinline__ u64 st_load(const u64 *p) {
 // a time and returns the exclusive prefix (all lanes).  A wait that exceeds
 // SPIN_LIMIT polls sets ERR_TIMEOUT and proceeds with what it has, so a lost
 // predecessor can never hang the GPU.
-__device__ __forceinline__ unsigned lookback_warp(u64 *status, int tile, unsigned epoch, unsigned agg, int *err) {
+__device__ __forceinline__ unsigned lookback_warp(u64 *status, int tile, unsigned epoch, unsigned agg, int *err,
+                                                  long long limit = SPIN_LIMIT) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
         if (lane == 0) st_publish(status, st_make(ST_PRE, epoch, agg));
@@ -204,7 +205,7 @@ __device__ __forceinline__ unsigned lookback_warp(u64 *status, int tile, unsigne
         int fp = pre ? (__ffs(pre) - 1) : 31;
         unsigned need = fp == 31 ? 0xffffffffu : ((2u << fp) - 1u);
         if ((rdy & need) != need) {
-            if (++spins > SPIN_LIMIT) {
+            if (++spins > limit) {
                 if (lane == 0) atomicOr(err, ERR_TIMEOUT);
                 break;
             }

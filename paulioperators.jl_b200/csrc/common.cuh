@@ -88,6 +88,10 @@ struct DevState {
     int measure_valid;
     int seg_dense;                // 0: live set cur is the last window-1 merge's per-tile slots (segment table)
     int pad;
+    long long bk_rot0;            // bucketed rotations: first rotation of the launched group
+    long long bk_fail;            // bucketed rotations: first rotation whose output overflowed a bucket
+    int bk_cur0;                  // bucketed rotations: input bucket set of the group's first rotation
+    int bk_pad;
 };
 
 // Static per-kernel configuration.

@@ -73,6 +73,10 @@ class PPDropSample(Structure):
                 ("n", c_int64), ("n_dropped", c_int64)]
 
 
+class PPTuning(Structure):
+    _fields_ = [("bucket_cap", c_int32), ("items_per_thread", c_int32), ("load_div", c_int32), ("chunk", c_int32)]
+
+
 PP_MLP_NPARAM = 5313
 PP_STATS_LEN = 16
 STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
@@ -124,6 +128,10 @@ SIGNATURES = {
     "pp_inner_product": (c_int32, [c_void_p, c_void_p, POINTER(c_double)]),
     "pp_product": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32]),
     "pp_last_error": (c_char_p, []),
+    "pp_set_tuning": (c_int32, [c_void_p, POINTER(PPTuning)]),
+    "pp_get_tuning": (c_int32, [c_void_p, POINTER(PPTuning)]),
+    "pp_debug_fail_alloc": (c_int32, [c_int64]),
+    "pp_debug_lookback_timeout": (c_int32, [c_int64]),
 }
 
 

@@ -55,7 +55,8 @@ def test_struct_layouts():
     import tempfile
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     structs = {"pp_filter": _lib.PPFilter, "pp_evolve_opts": _lib.PPEvolveOpts, "pp_counters": _lib.PPCounters,
-               "pp_batch": _lib.PPBatch, "pp_feature_ctx": _lib.PPFeatureCtx, "pp_drop_sample": _lib.PPDropSample}
+               "pp_batch": _lib.PPBatch, "pp_feature_ctx": _lib.PPFeatureCtx, "pp_drop_sample": _lib.PPDropSample,
+               "pp_tuning": _lib.PPTuning}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pauliprop.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

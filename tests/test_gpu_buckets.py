@@ -1,0 +1,222 @@
+"""Window-1 rotations on the hash-bucketed live set (k_bk_rotate) against the CPU
+oracle, and against the sorted-merge kernels on the same inputs.
+
+Sequences of at least 32 rotations over live sets above k_small_run's size run on
+buckets.  Bar: bit-exact key sets and bit-identical coefficients (window 1: each
+output sums at most two separately rounded products, so the bucketed order of
+the partners cannot change a bit), per-rotation WindowCounters equal to the
+oracle's (spv_evolve.jl:149-161), and <ket|O|ket> within 1e-12 * sum_{x=0}|c|.
+The cases cover one- and two-word keys, one- to many-qubit generators (whose
+bucket partner is another bucket or the same one), the early-merge pre-filter
+(spv_evolve.jl:356-362), local truncation, channels fused at layer ends, growth
+that splits the buckets in the middle of a call, and every compiled launch
+variant (pp_set_tuning)."""
+import ctypes
+import os
+import random
+
+import numpy as np
+import pytest
+
+import orc
+import pauliprop as pp
+from helpers import CHANNEL_KIND, filt, rand_terms, strategy
+from pauliprop import _lib
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [(256, 2), (256, 4), (512, 2), (512, 4), (1024, 4), (1024, 8)]
+
+
+def _gens(rng, N, L):
+    gens, angs = [], []
+    for _ in range(L):
+        q = rng.sample(range(N), 3)
+        kind = rng.randrange(6)
+        if kind == 0:
+            gens.append(((1 << q[0]) | (1 << q[1]), 0))                       # ZZ
+        elif kind == 1:
+            gens.append((0, 1 << q[0]))                                       # X
+        elif kind == 2:
+            gens.append((1 << q[0], 1 << q[0]))                               # Y
+        elif kind == 3:
+            gens.append(((1 << q[0]) | (1 << q[2]), (1 << q[1]) | (1 << q[2])))   # Z X Y
+        elif kind == 4:
+            gens.append((1 << q[0], 0))                                       # Z
+        else:
+            m = (1 << N) - 1
+            gens.append((rng.getrandbits(N) & m, rng.getrandbits(N) & m))     # dense string
+        angs.append(rng.uniform(-1.5, 1.5))
+    return gens, angs
+
+
+def _oracle(N, terms, **kw):
+    return orc.OracleSPV.from_terms(N, [(k[0], k[1], c) for k, c in terms.items()], **kw)
+
+
+def _gpu(v, N, tuning=None):
+    z, x, c = v.arrays()
+    g = pp.SparsePauliVector(N, max(16, 2 * len(c)), v.append_cap)
+    g.upload(z, x, c, sorted=True)
+    if tuning:
+        _lib.check(_lib.lib.pp_set_tuning(g._h, ctypes.byref(_lib.PPTuning(*tuning))))
+    return g
+
+
+def _same(g, v):
+    gz, gx, gc = g.to_arrays()
+    oz, ox, oc = v.arrays()
+    assert gz.shape == oz.shape, (gz.shape, oz.shape)
+    assert np.array_equal(gz, oz) and np.array_equal(gx, ox), "key sets differ"
+    assert np.array_equal(gc.view(np.uint64), oc.view(np.uint64)), "coefficients not bit-identical"
+    pp.check_spv(g)
+
+
+def _on(path, fn):
+    old = os.environ.get("PAULIPROP_WINDOW1_PATH")
+    os.environ["PAULIPROP_WINDOW1_PATH"] = path
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ["PAULIPROP_WINDOW1_PATH"]
+        else:
+            os.environ["PAULIPROP_WINDOW1_PATH"] = old
+
+
+@pytest.mark.parametrize("N", [30, 64, 100])
+@pytest.mark.parametrize("spec", [("coeff", 1e-6), ("comp", [("coeff", 1e-7), ("weight", 20)])], ids=str)
+def test_bucket_random_sequences(N, spec):
+    rng = random.Random(7 * N)
+    terms = rand_terms(rng, N, 20_000)
+    gens, angs = _gens(rng, N, 48)
+    v = _oracle(N, terms)
+    g = _gpu(v, N)
+    t = _gpu(v, N)
+    _, ctr = v.evolve(gens, angs, window=1, strict=filt(spec), nwin=len(gens))
+    wc = pp.WindowCounters(len(gens))
+    G = [pp.PauliBasis(N, a, b) for a, b in gens]
+    _, e = _on("buckets", lambda: pp.evolve_(g, G, angs, truncation=strategy(spec), counters=wc,
+                                             return_expectation=True))
+    _same(g, v)
+    assert np.array_equal(wc.terms_created, ctr[0])
+    assert np.array_equal(wc.merge_in, ctr[1])
+    assert np.array_equal(wc.merge_out, ctr[2])
+    z, x, c = v.arrays()
+    diag = np.all(x == 0, axis=1)
+    assert abs(e - v.expect(0)) <= 1e-12 * max(1e-300, float(np.abs(c[diag]).sum()))
+    # the sorted-merge kernels on the same input give the same vector
+    _on("tiles", lambda: pp.evolve_(t, G, angs, truncation=strategy(spec)))
+    _same(t, v)
+
+
+@pytest.mark.parametrize("variant", VARIANTS, ids=str)
+def test_bucket_every_variant(variant):
+    """Every compiled (bucket capacity, items per thread) launch variant, with small
+    load divisors and chunks, gives the oracle's vector bit for bit."""
+    rng = random.Random(sum(variant))
+    for N in (64, 90):
+        terms = rand_terms(rng, N, 8_000)
+        gens, angs = _gens(rng, N, 40)
+        spec = ("coeff", 1e-6)
+        v = _oracle(N, terms)
+        g = _gpu(v, N, tuning=(variant[0], variant[1], 3, 8))
+        tn = _lib.PPTuning()
+        _lib.check(_lib.lib.pp_get_tuning(g._h, ctypes.byref(tn)))
+        assert (tn.bucket_cap, tn.items_per_thread, tn.load_div, tn.chunk) == (variant[0], variant[1], 3, 8)
+        v.evolve(gens, angs, window=1, strict=filt(spec))
+        _on("buckets", lambda: pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs,
+                                          truncation=strategy(spec)))
+        _same(g, v)
+
+
+def test_tuning_argument_errors():
+    g = pp.SparsePauliVector(8)
+    for bad in ((384, 4, 5, 64), (512, 3, 5, 64), (512, 4, 2, 64), (512, 4, 5, 4), (512, 4, 5, 512)):
+        assert _lib.lib.pp_set_tuning(g._h, ctypes.byref(_lib.PPTuning(*bad))) == _lib.PP_ARGUMENT_ERROR
+
+
+def test_bucket_early_merge_prefilter():
+    """A small append capacity makes n > capacity, so rotations start with the
+    early boundary that filters live terms before rotating (pre-filtered terms
+    come back as new sin branches of their live partners)."""
+    rng = random.Random(11)
+    N = 40
+    terms = rand_terms(rng, N, 12_000)
+    for k in list(terms)[:4000]:
+        terms[k] = 1e-9 * (rng.random() - 0.5)       # below the threshold before any rotation
+    gens, angs = _gens(rng, N, 40)
+    spec = ("coeff", 1e-6)
+    v = _oracle(N, terms, append_factor=0.05, min_capacity=4)
+    g = _gpu(v, N)
+    _, ctr = v.evolve(gens, angs, window=1, strict=filt(spec), nwin=len(gens))
+    assert ctr[3].sum() > 0
+    wc = pp.WindowCounters(len(gens))
+    _on("buckets", lambda: pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs,
+                                      truncation=strategy(spec), counters=wc))
+    _same(g, v)
+    assert np.array_equal(wc.early_merges, ctr[3])
+    assert np.array_equal(wc.merge_in, ctr[1])
+    assert np.array_equal(wc.merge_out, ctr[2])
+
+
+@pytest.mark.parametrize("N", [50, 90])
+def test_bucket_local_truncation_and_channel(N):
+    rng = random.Random(3 + N)
+    terms = rand_terms(rng, N, 15_000)
+    gens, angs = _gens(rng, N, 36)
+    spec, lspec = ("comp", [("coeff", 1e-6), ("weight", 3 * N // 4 + 4)]), ("coeff", 2e-4)
+    per = 12
+    v = _oracle(N, terms)
+    g = _gpu(v, N)
+    for s in range(0, len(gens), per):
+        v.evolve(gens[s:s + per], angs[s:s + per], window=1, strict=filt(spec), local=filt(lspec))
+        v.channel(CHANNEL_KIND["depolarizing"], [0.01])
+    _on("buckets", lambda: pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs, truncation=strategy(spec),
+                                      local_truncation=strategy(lspec), channel=("depolarizing", 0.01, None),
+                                      channel_every=per))
+    _same(g, v)
+
+
+@pytest.mark.parametrize("N", [64, 120])
+def test_bucket_growth_splits(N):
+    """From 2,500 terms the set grows by orders of magnitude within one call, so
+    buckets overflow or pass their split size in the middle of launched chunks."""
+    rng = random.Random(N)
+    terms = rand_terms(rng, N, 2500)
+    gens, angs = [], []
+    for _ in range(96):
+        i, j = rng.sample(range(N // 2), 2)
+        gens.append(((1 << i) | (1 << j), 0) if rng.random() < 0.6 else (0, 1 << i))
+        angs.append(rng.uniform(0.2, 1.2))
+    spec = ("coeff", 1e-5)
+    v = _oracle(N, terms)
+    g = _gpu(v, N)
+    v.evolve(gens, angs, window=1, strict=filt(spec))
+    _on("buckets", lambda: pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs, truncation=strategy(spec)))
+    assert len(v) > 20 * 2500
+    _same(g, v)
+
+
+def test_bucket_config2_whole_circuit():
+    """The 8x8-lattice benchmark circuit (3,520 rotations, peak 3.9e6 terms) in one
+    call on buckets, bit for bit against the oracle."""
+    w = pp.circuits.lattice64()
+    f = filt(("comp", [("coeff", w.thresh), ("weight", w.wmax)]))
+    v = orc.OracleSPV.from_terms(w.N, w.observable)
+    gens1 = [(p.z, p.x) for p in w.layer]
+    for _ in range(w.layers):
+        v.evolve(gens1, w.angles, window=1, strict=f)
+        v.channel(CHANNEL_KIND[w.channel[0]], [w.channel[1]])
+    ps = pp.PauliSum(w.N)
+    for z, x, c in w.observable:
+        ps[(z, x)] = c
+    g = pp.SparsePauliVector.from_paulisum(ps)
+    gens, angs = w.generators()
+    _, e = _on("buckets", lambda: pp.evolve_(
+        g, gens, angs, truncation=strategy(("comp", [("coeff", w.thresh), ("weight", w.wmax)])),
+        channel=(w.channel[0], w.channel[1], None), channel_every=len(w.layer), return_expectation=True))
+    _same(g, v)
+    z, x, c = v.arrays()
+    diag = np.all(x == 0, axis=1)
+    assert abs(e - v.expect(0)) <= 1e-12 * max(1e-300, float(np.abs(c[diag]).sum()))

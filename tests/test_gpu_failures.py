@@ -1,0 +1,99 @@
+"""Failure detection without a GPU fault (the reference models capacity exhaustion
+by forcing tiny buffers, test_spv_evolution.jl:154-167, and grows and retries,
+spv_evolve.jl:356-362, spv_kernels.jl:377-386).
+
+- Allocation failure, injected on the host (pp_debug_fail_alloc): whichever
+  device allocation of an evolve! call fails -- a live-set growth, the bucket
+  sets, a workspace -- the call reports PP_OUT_OF_MEMORY (MemoryError) and the
+  handle keeps its previous live set, bit for bit; with the injection off the
+  same call then matches the oracle.  Both window-1 paths are covered.
+- A bounded device wait that runs out: a look-back on a status nothing publishes
+  gives up after its poll limit, the host gets PP_TIMEOUT (TimeoutError), and the
+  device keeps answering."""
+import os
+import random
+
+import numpy as np
+import pytest
+
+import orc
+import pauliprop as pp
+from helpers import filt, rand_terms, strategy
+from pauliprop import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _gens(rng, N, L):
+    gens, angs = [], []
+    for _ in range(L):
+        i, j = rng.sample(range(N), 2)
+        gens.append(((1 << i) | (1 << j), 0) if rng.random() < 0.6 else (0, 1 << i))
+        angs.append(rng.uniform(0.2, 1.2))
+    return gens, angs
+
+
+@pytest.mark.parametrize("path", ["tiles", "buckets"])
+@pytest.mark.parametrize("after", [1, 2, 3, 5, 8, 13, 21, 30, 40, 50, 60])
+def test_injected_allocation_failure_leaves_handle_usable(after, path):
+    rng = random.Random(after)
+    N = 64
+    terms = rand_terms(rng, N, 5000)
+    keys = sorted(terms)
+    z, x = pp.pack_keys(N, keys)
+    c = np.array([terms[k] for k in keys])
+    gens, angs = _gens(rng, N, 64)
+    G = [pp.PauliBasis(N, a, b) for a, b in gens]
+    spec = ("coeff", 1e-5)
+    old = os.environ.get("PAULIPROP_WINDOW1_PATH")
+    os.environ["PAULIPROP_WINDOW1_PATH"] = path
+    try:
+        g = pp.SparsePauliVector(N, 5000, 5000)     # room for the input only: the call must grow
+        g.upload(z, x, c, sorted=True)
+        _lib.check(_lib.lib.pp_debug_fail_alloc(after))
+        failed = False
+        try:
+            pp.evolve_(g, G, angs, truncation=strategy(spec))
+        except MemoryError as e:
+            failed = True
+            assert "injected" in str(e)
+        finally:
+            _lib.check(_lib.lib.pp_debug_fail_alloc(0))
+        if failed:
+            gz, gx, gc = g.to_arrays()
+            assert np.array_equal(gz, z) and np.array_equal(gx, x)
+            assert np.array_equal(gc.view(np.uint64), c.view(np.uint64))
+            pp.check_spv(g)
+            pp.evolve_(g, G, angs, truncation=strategy(spec))
+    finally:
+        if old is None:
+            del os.environ["PAULIPROP_WINDOW1_PATH"]
+        else:
+            os.environ["PAULIPROP_WINDOW1_PATH"] = old
+    v = orc.OracleSPV(N, 16, 16)
+    v.upload(z, x, c)
+    v.evolve(gens, angs, window=1, strict=filt(spec))
+    gz, gx, gc = g.to_arrays()
+    oz, ox, oc = v.arrays()
+    assert np.array_equal(gz, oz) and np.array_equal(gx, ox)
+    assert np.array_equal(gc.view(np.uint64), oc.view(np.uint64))
+
+
+def test_bounded_wait_times_out_and_device_answers():
+    st = _lib.lib.pp_debug_lookback_timeout(2000)
+    assert st == _lib.PP_TIMEOUT
+    with pytest.raises(TimeoutError):
+        _lib.check(st)
+    assert _lib.lib.pp_debug_lookback_timeout(0) == _lib.PP_ARGUMENT_ERROR
+    # the context is intact: a small evolve! still matches the oracle
+    N = 8
+    v = orc.OracleSPV.from_terms(N, [(1 << 3, 0, 1.0)])
+    g = pp.SparsePauliVector(N)
+    g.upload(*v.arrays(), sorted=True)
+    gens = [(0b11 << k, 0) for k in range(7)] + [(0, 1 << k) for k in range(8)]
+    angs = [0.3] * 7 + [0.2] * 8
+    v.evolve(gens, angs, window=1)
+    pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs)
+    gz, gx, gc = g.to_arrays()
+    oz, ox, oc = v.arrays()
+    assert np.array_equal(gz, oz) and np.array_equal(gc.view(np.uint64), oc.view(np.uint64))
