@@ -310,6 +310,9 @@ typedef struct {
 } pp_tuning;
 int pp_set_tuning(pp_spv *h, const pp_tuning *t);
 int pp_get_tuning(pp_spv *h, pp_tuning *t);
+/* The handle's device: multiprocessor count and compute capability (the key of the
+ * tuning cache). */
+int pp_device_info(pp_spv *h, int32_t *sm_count, int32_t *cc_major, int32_t *cc_minor);
 
 /* Test hooks for failure detection (no counterpart in the reference, which has no
  * device).  pp_debug_fail_alloc: the after-th next device allocation of any handle

@@ -1934,6 +1934,17 @@ extern "C" int pp_get_tuning(pp_spv *h, pp_tuning *t) {
     return PP_OK;
 }
 
+extern "C" int pp_device_info(pp_spv *h, int32_t *sm_count, int32_t *cc_major, int32_t *cc_minor) {
+    if (!h || !sm_count || !cc_major || !cc_minor) return fail(PP_ARGUMENT_ERROR, "pp_device_info: null argument");
+    int ma = 0, mi = 0;
+    CU(cudaDeviceGetAttribute(&ma, cudaDevAttrComputeCapabilityMajor, h->dev));
+    CU(cudaDeviceGetAttribute(&mi, cudaDevAttrComputeCapabilityMinor, h->dev));
+    *sm_count = h->nsm;
+    *cc_major = ma;
+    *cc_minor = mi;
+    return PP_OK;
+}
+
 // ------------------------------------------------------------------ test hooks
 extern "C" int pp_debug_fail_alloc(int64_t after) {
     g_fail_alloc_after.store(after > 0 ? after : 0);

@@ -37,7 +37,7 @@ _DEVICE_NAMES = {
     "_lib": ("LIB_PATH",),
 }
 _LAZY = {name: mod for mod, names in _DEVICE_NAMES.items() for name in names}
-_LAZY_MODULES = ("spv", "batch", "learned", "_lib")
+_LAZY_MODULES = ("spv", "batch", "learned", "_lib", "tune")
 
 
 def __getattr__(name):

@@ -130,6 +130,7 @@ SIGNATURES = {
     "pp_last_error": (c_char_p, []),
     "pp_set_tuning": (c_int32, [c_void_p, POINTER(PPTuning)]),
     "pp_get_tuning": (c_int32, [c_void_p, POINTER(PPTuning)]),
+    "pp_device_info": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
     "pp_debug_fail_alloc": (c_int32, [c_int64]),
     "pp_debug_lookback_timeout": (c_int32, [c_int64]),
 }

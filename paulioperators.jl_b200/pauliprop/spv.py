@@ -70,6 +70,8 @@ class SparsePauliVector:
         h = c_void_p()
         check(lib.pp_create(self.N, cap, acap, byref(h)))
         self._h = h
+        from .tune import apply_cached
+        apply_cached(self)          # the autotuned launch configuration of this device, if cached
 
     # -- construction / conversion ------------------------------------------
     @classmethod

@@ -1,0 +1,152 @@
+"""Autotuner of the bucketed window-1 rotations (no counterpart in the reference).
+
+The launch configuration of k_bk_rotate -- bucket capacity (the CTA's tile of
+terms), items per thread, the bucketing load divisor and the rotations launched
+between host checks -- changes how fast a sequence runs, never what it computes
+(every variant is checked bit for bit against the oracle in the GPU tests).
+`tune()` times each candidate on the device on a representative sequence per
+word count and writes the fastest to a JSON cache keyed by the device's SM count
+and compute capability; `apply_cached(v)` gives a new vector the cached setting.
+
+Cache file: paulioperators.jl_b200/tuning/sm<count>_cc<major><minor>.json
+  {"sm_count": 148, "cc": [10, 0],
+   "nw": {"1": {"tuning": [cap, items, load_div, chunk], "terms_per_s": ..., "workload": "..."},
+          "2": {...}},
+   "candidates": {"1": [[cap, items, load_div, chunk, terms_per_s], ...], "2": [...]}}
+
+Run on the target GPU:  python -m pauliprop.tune [--quick]
+"""
+import ctypes
+import json
+import os
+import sys
+import time
+
+from . import _lib
+from .circuits import lattice64
+
+TUNING_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tuning")
+VARIANTS = [(256, 2), (256, 4), (512, 2), (512, 4), (1024, 4), (1024, 8)]
+LOAD_DIVS = (4, 5, 6)
+CHUNKS = (32, 64, 128)
+DEFAULT = (512, 4, 5, 64)
+
+_cache = {}
+
+
+def device_info(v):
+    sm, ma, mi = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    _lib.check(_lib.lib.pp_device_info(v._h, ctypes.byref(sm), ctypes.byref(ma), ctypes.byref(mi)))
+    return sm.value, ma.value, mi.value
+
+
+def cache_path(sm, ma, mi):
+    return os.path.join(TUNING_DIR, f"sm{sm}_cc{ma}{mi}.json")
+
+
+def set_tuning(v, t):
+    _lib.check(_lib.lib.pp_set_tuning(v._h, ctypes.byref(_lib.PPTuning(*t))))
+
+
+def get_tuning(v):
+    t = _lib.PPTuning()
+    _lib.check(_lib.lib.pp_get_tuning(v._h, ctypes.byref(t)))
+    return (t.bucket_cap, t.items_per_thread, t.load_div, t.chunk)
+
+
+def cached(sm, ma, mi, nw):
+    """The cached tuning for (device, word count), or None."""
+    key = (sm, ma, mi)
+    if key not in _cache:
+        try:
+            with open(cache_path(sm, ma, mi)) as f:
+                _cache[key] = json.load(f)
+        except (OSError, ValueError):
+            _cache[key] = None
+    d = _cache[key]
+    if not d:
+        return None
+    e = d.get("nw", {}).get(str(nw))
+    return tuple(e["tuning"]) if e else None
+
+
+def apply_cached(v):
+    """Gives vector v the cached tuning of its device and word count (if any)."""
+    t = cached(*device_info(v), v.nw)
+    if t:
+        set_tuning(v, t)
+    return t
+
+
+def _workload(nw):
+    """The 8x8-lattice benchmark circuit (3,520 rotations); for two-word keys the
+    same terms declared on 100 qubits."""
+    w = lattice64()
+    return w, (64 if nw == 1 else 100)
+
+
+def _time_one(nw, t, reps):
+    from . import spv
+    from .paulis import PauliSum, PauliBasis
+    from .truncation import CoeffTruncation, CompositeTruncation, WeightTruncation
+    w, N = _workload(nw)
+    ps = PauliSum(N)
+    for z, x, c in w.observable:
+        ps[(z, x)] = c
+    gens = [PauliBasis(N, p.z, p.x) for p in w.layer] * w.layers
+    angs = list(w.angles) * w.layers
+    strat = CompositeTruncation(CoeffTruncation(w.thresh), WeightTruncation(w.wmax))
+    best = None
+    for _ in range(reps + 1):     # the first run warms up (allocations, graphs)
+        v = spv.SparsePauliVector.from_paulisum(ps)
+        set_tuning(v, t)
+        st = {}
+        t0 = time.perf_counter()
+        spv.evolve_(v, gens, angs, truncation=strat, channel=(w.channel[0], w.channel[1], None),
+                    channel_every=len(w.layer), stats=st)
+        dt = time.perf_counter() - t0
+        rate = st["terms_in"] / dt
+        best = rate if best is None or rate > best else best
+        v.close()
+    return best
+
+
+def tune(nws=(1, 2), quick=False, reps=2, log=print):
+    """Measures the candidates and writes the cache; returns its dict."""
+    os.environ["PAULIPROP_WINDOW1_PATH"] = "buckets"
+    from . import spv
+    probe = spv.SparsePauliVector(8)
+    sm, ma, mi = device_info(probe)
+    probe.close()
+    out = {"sm_count": sm, "cc": [ma, mi], "nw": {}, "candidates": {}}
+    for nw in nws:
+        cands = []
+        # variants at the default load divisor and chunk, then the best variant's
+        # load divisor and chunk
+        for cap, items in (VARIANTS if not quick else [(512, 4), (1024, 4)]):
+            t = (cap, items, DEFAULT[2], DEFAULT[3])
+            cands.append((t, _time_one(nw, t, reps)))
+            log(f"nw={nw} {t}: {cands[-1][1]:.4g} terms/s")
+        cap, items = max(cands, key=lambda c: c[1])[0][:2]
+        for ld in LOAD_DIVS:
+            for ch in (CHUNKS if not quick else (64,)):
+                t = (cap, items, ld, ch)
+                if any(c[0] == t for c in cands):
+                    continue
+                cands.append((t, _time_one(nw, t, reps)))
+                log(f"nw={nw} {t}: {cands[-1][1]:.4g} terms/s")
+        best = max(cands, key=lambda c: c[1])
+        w, N = _workload(nw)
+        out["nw"][str(nw)] = {"tuning": list(best[0]), "terms_per_s": best[1],
+                              "workload": f"{w.name} circuit on N={N} ({w.layers} layers x {len(w.layer)} rotations)"}
+        out["candidates"][str(nw)] = [list(t) + [r] for t, r in cands]
+    os.makedirs(TUNING_DIR, exist_ok=True)
+    with open(cache_path(sm, ma, mi), "w") as f:
+        json.dump(out, f, indent=1)
+    _cache.pop((sm, ma, mi), None)
+    return out
+
+
+if __name__ == "__main__":
+    res = tune(quick="--quick" in sys.argv)
+    print(json.dumps(res["nw"]))

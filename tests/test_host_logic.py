@@ -85,3 +85,19 @@ def test_trotterize_order2():
     g, a = circuits.trotterize(terms, 0.1, n_trotter=2, order=2)
     assert len(g) == 2 * 2 * len(terms)
     assert g[len(terms)] == terms[-1][0] and a[0] == pytest.approx(0.05 * terms[0][1])
+
+
+def test_tuning_cache_lookup(tmp_path, monkeypatch):
+    """The autotuner's cache is keyed by SM count and compute capability, per word count."""
+    import json
+    from pauliprop import tune
+    monkeypatch.setattr(tune, "TUNING_DIR", str(tmp_path))
+    tune._cache.clear()
+    assert tune.cached(148, 10, 0, 1) is None
+    (tmp_path / "sm148_cc100.json").write_text(json.dumps(
+        {"sm_count": 148, "cc": [10, 0], "nw": {"1": {"tuning": [1024, 4, 5, 64], "terms_per_s": 1.0}}}))
+    tune._cache.clear()
+    assert tune.cached(148, 10, 0, 1) == (1024, 4, 5, 64)
+    assert tune.cached(148, 10, 0, 2) is None
+    assert tune.cached(132, 9, 0, 1) is None
+    tune._cache.clear()
