@@ -60,6 +60,8 @@ BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
 # dram__bytes_write.sum = 115.1 MB per launch against B(n + a + m) = 150.9 MB:
 # the gathered sin branches re-read live terms that are still in L2)
 MERGE_TRAFFIC_PER_ALG_BYTE = 115.09 / 150.88
+# DRAM traffic of k_bk_rotate per algorithmic byte: not captured yet
+BUCKET_TRAFFIC_PER_ALG_BYTE = None
 
 
 def parse():
@@ -674,12 +676,23 @@ def run_ours(args):
     t_e2e = reduce_max(sum(te), ws, dev)
     e2e_value = total_terms / t_e2e
 
-    # profiled pass: per-kernel device time for the roofline of the merge kernel
+    # profiled pass: per-kernel device time for the roofline of the dominant kernel
     sp = {}
     one_step(stats=sp, profile=True)
-    merge_bytes = B * (sp["merge_in"] + sp["merge_out"])          # B*(n + a + m) per launch, summed
-    achieved = merge_bytes / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
     pipe_bytes = B * (sp["terms_in"] + sp["merge_out"])          # B*(n + m) per rotation, summed
+    tuning = pp.tune.get_tuning(g)
+    if sp["bucket_rot"] > 0:
+        # bucketed rotations: one k_bk_rotate launch per rotation reads its n live
+        # terms and writes its m survivors, B*(n + m) per launch
+        dom_bytes, dom_launches = sp["bucket_bytes"], sp["bucket_rot"]
+        dom_kernel = (f"k_bk_rotate<{nw},{tuning[0]},{tuning[1]}> (rotation + partner merge + filter + "
+                      f"channel over bucket pairs)")
+        traffic_ratio = BUCKET_TRAFFIC_PER_ALG_BYTE
+    else:
+        dom_bytes, dom_launches = B * (sp["merge_in"] + sp["merge_out"]), len(gens)   # B*(n + a + m)
+        dom_kernel = "k_merge<1,0> (merge + reduce-by-key + filter + channel + compaction)"
+        traffic_ratio = MERGE_TRAFFIC_PER_ALG_BYTE if w.name == "lattice64" else None
+    achieved = dom_bytes / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
     hbm, src = peaks()
 
     # CPU baseline (the concurrent whole-circuit oracle run) and the final check
@@ -722,16 +735,19 @@ def run_ours(args):
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None,
-                         "traffic": (MERGE_TRAFFIC_PER_ALG_BYTE * merge_bytes / max(1.0, len(gens))
-                                     if w.name == "lattice64" else None),
-                         "traffic_unit": "bytes per merge launch (ncu-measured ratio x this step's mean "
-                                         "algorithmic bytes per launch)",
-                         "alg_bytes_per_launch": merge_bytes / max(1.0, len(gens)),
-                         "kernel": "k_merge<1,0> (merge + reduce-by-key + filter + channel + compaction)",
+                         "traffic": (traffic_ratio * dom_bytes / max(1.0, dom_launches)
+                                     if traffic_ratio and w.name == "lattice64" else None),
+                         "traffic_unit": "bytes per launch of the kernel (ncu-measured DRAM bytes per "
+                                         "algorithmic byte x this step's mean algorithmic bytes per launch)",
+                         "alg_bytes_per_launch": dom_bytes / max(1.0, dom_launches),
+                         "kernel": dom_kernel, "launches_per_step": dom_launches,
                          "peak_source": src,
-                         "pipeline_frac": pipe_bytes / (sp["t_rotate"] + sp["t_merge"] + sp["t_partition"]) / 1e9 / hbm,
-                         "t_merge_s": sp["t_merge"], "t_rotate_s": sp["t_rotate"],
+                         "pipeline_frac": pipe_bytes / (t / args.steps) / 1e9 / hbm,
+                         "pipeline_frac_is": "B*(n + m) summed over the step's rotations / the timed step time",
+                         "t_kernel_s": sp["t_merge"], "t_rotate_s": sp["t_rotate"],
                          "t_partition_commit_s": sp["t_partition"]},
+            "tuning": {"bucket_cap": tuning[0], "items_per_thread": tuning[1], "load_div": tuning[2],
+                       "chunk": tuning[3]},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -100,6 +100,8 @@ typedef struct {
 #define PP_STAT_T_MERGE 7         /* seconds in the merge kernel alone (profile = 1) */
 #define PP_STAT_LAUNCHES 8        /* kernels launched by the call */
 #define PP_STAT_T_PARTITION 9     /* seconds in partition + commit kernels (profile = 1) */
+#define PP_STAT_BUCKET_ROT 10     /* rotations run by the bucketed kernel (k_bk_rotate) */
+#define PP_STAT_BUCKET_BYTES 11   /* algorithmic bytes of those rotations: B * (terms in + terms out) */
 #define PP_STATS_LEN 16
 
 /* _alloc_spv (type_SparsePauliVector.jl:94-104) / SparsePauliVector(N, T; capacity)

@@ -799,6 +799,8 @@ struct RunProf {
     bool on = false;
     double t_rotate = 0, t_partition = 0, t_merge = 0;
     long long launches = 0;
+    long long bk_rot = 0;          // rotations run on buckets
+    double bk_bytes = 0;           // their algorithmic bytes B * (n_in + n_out)
 };
 
 // ------------------------------------------------------------------ bucketed window-1 rotations
@@ -1152,6 +1154,8 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
         st.merge_out += tot;
         if (tot > st.peak) st.peak = tot;
         if (o.pref) st.early += 1;
+        prof->bk_rot += 1;
+        prof->bk_bytes += (double)(16 * NW + 8) * (double)(n + tot);
         if (h->rec_on) {
             // WindowCounters of the rotation (window = 1): an early boundary merges
             // n -> np first, the regular one np + a -> total
@@ -1804,6 +1808,8 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
         so[PP_STAT_T_ROTATE] = prof.t_rotate;
         so[PP_STAT_T_MERGE] = prof.t_merge;
         so[PP_STAT_LAUNCHES] = (double)prof.launches;
+        so[PP_STAT_BUCKET_ROT] = (double)prof.bk_rot;
+        so[PP_STAT_BUCKET_BYTES] = prof.bk_bytes;
         so[PP_STAT_T_PARTITION] = prof.t_partition;
     }
     return PP_OK;
@@ -2156,6 +2162,8 @@ static int batch_impl(pp_spv *h, const void *gz, const void *gx, long long L, co
         so[PP_STAT_T_ROTATE] = prof.t_rotate;
         so[PP_STAT_T_MERGE] = prof.t_merge;
         so[PP_STAT_LAUNCHES] = (double)prof.launches;
+        so[PP_STAT_BUCKET_ROT] = (double)prof.bk_rot;
+        so[PP_STAT_BUCKET_BYTES] = prof.bk_bytes;
         so[PP_STAT_T_PARTITION] = prof.t_partition;
     }
     return PP_OK;

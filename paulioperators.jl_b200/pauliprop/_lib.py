@@ -80,7 +80,7 @@ class PPTuning(Structure):
 PP_MLP_NPARAM = 5313
 PP_STATS_LEN = 16
 STAT = {"terms_in": 0, "created": 1, "merge_in": 2, "merge_out": 3, "peak": 4, "early": 5,
-        "t_rotate": 6, "t_merge": 7, "launches": 8, "t_partition": 9}
+        "t_rotate": 6, "t_merge": 7, "launches": 8, "t_partition": 9, "bucket_rot": 10, "bucket_bytes": 11}
 
 
 # Every symbol include/pauliprop.h declares, with its ctypes signature.
