@@ -818,18 +818,18 @@ static bool bk_enabled() {
     return e && strcmp(e, "buckets") == 0;
 }
 
-// Compiled variants of k_bk_rotate: (bucket capacity, items per thread).
+// Compiled variants of k_bk_rotate: (bucket capacity, staged items per thread).
 typedef void (*BkKernel)(BkArgs, int);
 struct BkVariant {
-    int cap, items, threads;
+    int cap, items, gmax;
     BkKernel k1, k2;
     size_t smem1, smem2;
 };
-#define PP_BK_VARIANT(C, I)                                                                              \
-    { C, I, bk_threads<C, I>(), k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, bk_smem_bytes<1, C>(),       \
-      bk_smem_bytes<2, C>() }
-static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(256, 2), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(512, 2),
-                                        PP_BK_VARIANT(512, 4), PP_BK_VARIANT(1024, 4), PP_BK_VARIANT(1024, 8)};
+#define PP_BK_VARIANT(C, I)                                                                                 \
+    { C, I, bk_group_max<C, I>(), k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, bk_smem_bytes<1, C, I>(),     \
+      bk_smem_bytes<2, C, I>() }
+static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(128, 4), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(256, 8),
+                                        PP_BK_VARIANT(512, 8), PP_BK_VARIANT(512, 16), PP_BK_VARIANT(1024, 16)};
 #undef PP_BK_VARIANT
 
 static const BkVariant *bk_variant(int cap, int items) {
@@ -838,9 +838,19 @@ static const BkVariant *bk_variant(int cap, int items) {
     return nullptr;
 }
 
+// Bucket pairs per CTA for 2^bits buckets: as many as the variant stages, but
+// small enough to give every SM a few CTAs.
+static int bk_group_for(pp_spv *h, const BkVariant *v, int bits) {
+    const long long pairs = 1ll << (bits - 1);
+    int gsz = 1;
+    while (gsz * 2 <= v->gmax && pairs / (gsz * 2) >= 4ll * h->nsm) gsz *= 2;
+    return gsz;
+}
+
 template <int NW>
-static void bk_launch(pp_spv *h, const BkVariant *v, int bits, const BkArgs &A, int k) {
-    (NW == 1 ? v->k1 : v->k2)<<<1 << (bits - 1), v->threads, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
+static void bk_launch(pp_spv *h, const BkVariant *v, const BkArgs &A, int k) {
+    const int grid = (int)((1ll << (A.bits - 1)) / A.group);
+    (NW == 1 ? v->k1 : v->k2)<<<grid, BK_THREADS, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
 }
 
 // Hash rows: fixed pseudo-random words (splitmix64 from a fixed seed), so the
@@ -878,11 +888,12 @@ static int bk_bits_for(long long n, int cap, int load_div) {
     return b;
 }
 
-static BkArgs bk_args(pp_spv *h, int bits, BkRec *rec) {
+static BkArgs bk_args(pp_spv *h, const BkVariant *v, int bits, BkRec *rec) {
     BkArgs A;
     memset(&A, 0, sizeof A);
     for (int s = 0; s < 2; ++s) { A.z[s] = h->bkz[s]; A.x[s] = h->bkx[s]; A.c[s] = h->bkc[s]; A.cnt[s] = h->bkcnt[s]; }
     A.bits = bits;
+    A.group = bk_group_for(h, v, bits);
     A.rows = h->bk_rows;
     A.rec = rec;
     A.S = h->S;
@@ -1003,10 +1014,10 @@ static int bk_graph(pp_spv *h, const BkVariant *v, int bits, int cls, int len, c
     const int key = bits * 4 + cls;
     auto it = h->bk_graphs.find(key);
     if (it != h->bk_graphs.end()) { *out = it->second; return PP_OK; }
-    const BkArgs A = bk_args(h, bits, h->bk_rec);
+    const BkArgs A = bk_args(h, v, bits, h->bk_rec);
     cudaGraph_t graph = nullptr;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < len; ++k) bk_launch<NW>(h, v, bits, A, k);
+    for (int k = 0; k < len; ++k) bk_launch<NW>(h, v, A, k);
     CU(cudaStreamEndCapture(h->stream, &graph));
     cudaGraphExec_t ex = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
@@ -1102,13 +1113,13 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
                 r += cl;
             }
         } else {
-            const BkArgs A = bk_args(h, bits, h->bk_rec);
+            const BkArgs A = bk_args(h, var, bits, h->bk_rec);
             for (long long k = 0; k < len; ++k) {
                 cudaEvent_t e0, e1;
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, s);
-                bk_launch<NW>(h, var, bits, A, (int)k);
+                bk_launch<NW>(h, var, A, (int)k);
                 cudaEventRecord(e1, s);
                 TRY(sync_check(h));
                 float ms = 0.f;
@@ -1921,8 +1932,8 @@ extern "C" int pp_debug_phase_cycles(unsigned long long *out, int reset) {
 extern "C" int pp_set_tuning(pp_spv *h, const pp_tuning *t) {
     if (!h || !t) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: null argument");
     if (!bk_variant(t->bucket_cap, t->items_per_thread))
-        return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: (bucket_cap, items_per_thread) must be one of (256, 2), "
-                                       "(256, 4), (512, 2), (512, 4), (1024, 4), (1024, 8)");
+        return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: (bucket_cap, items_per_thread) must be one of (128, 4), "
+                                       "(256, 4), (256, 8), (512, 8), (512, 16), (1024, 16)");
     if (t->load_div < 3 || t->load_div > 16) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: load_div must be in 3..16");
     if (t->chunk < 8 || t->chunk > 256) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: chunk must be in 8..256");
     if (t->bucket_cap != h->tune.bucket_cap || t->items_per_thread != h->tune.items_per_thread ||

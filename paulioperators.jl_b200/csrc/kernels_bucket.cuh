@@ -14,11 +14,13 @@
 // pseudo-random rows R_r.  Linearity gives h(P xor M) = h(P) xor h(M), so for
 // the rotation's generator the partner of every term of bucket b lies in bucket
 // b xor delta, delta = h(M), and the sin branch of a term of b belongs to
-// b xor delta as well.  One CTA therefore owns one bucket pair {b, b xor delta}
-// (two neighbouring buckets when delta = 0): it loads both buckets into shared
-// memory, indexes their keys in a shared-memory hash table, finds each
-// anticommuting term's partner there, and writes both output buckets to the
-// other bucket set.  No cross-CTA scan, sort or wait is involved.
+// b xor delta as well.  A CTA therefore owns whole bucket pairs {b, b xor delta}
+// (two neighbouring buckets when delta = 0): it loads a group of pairs into
+// shared memory, indexes their keys in a shared-memory hash table, finds each
+// anticommuting term's partner there, and appends each output term to its
+// bucket of the other bucket set (positions from shared-memory counters, so the
+// order inside a bucket is arbitrary; nothing depends on it).  No cross-CTA
+// scan, sort or wait is involved.
 //
 // Per rotation, per term: the early-merge pre-filter, the cos branch, the sum
 // with the partner's sin branch (or a new term when the partner is absent or was
@@ -32,11 +34,15 @@
 namespace pp {
 
 // Compiled (bucket capacity, items per thread) variants; the autotuner picks
-// one per device.  A CTA holds one bucket pair: 2 * CAP terms, 2 * CAP / ITEMS
-// threads, and a key index of 4 * CAP slots (load at most 1/2).
+// one per device.  A CTA of BK_THREADS threads stages up to BK_THREADS * ITEMS
+// terms: a group of up to that many / CAP bucket pairs, processed in one pass
+// when their terms fit (else in consecutive sub-groups; a single pair always
+// fits, 2 * CAP <= BK_THREADS * ITEMS), with a shared-memory key index of twice
+// as many slots.
 constexpr int BK_ROWS = 26;                    // hash rows: at most 2^26 buckets
-constexpr int BK_DEFAULT_CAP = 512;
-constexpr int BK_DEFAULT_ITEMS = 4;
+constexpr int BK_THREADS = 256;
+constexpr int BK_DEFAULT_CAP = 256;
+constexpr int BK_DEFAULT_ITEMS = 8;
 
 // Per-rotation record: rec[r] describes the live set entering rotation r (the
 // output of rotation r - 1); rotation r reads it and fills rec[r + 1].
@@ -55,6 +61,7 @@ struct BkArgs {
     double *c[2];
     int *cnt[2];                    // terms per bucket
     int bits;                       // 2^bits buckets
+    int group;                      // bucket pairs per CTA (a power of two)
     const u64 *rows;                // [BK_ROWS][4]: z words 0..1, x words 0..1 of each hash row
     BkRec *rec;
     DevState *S;
@@ -86,27 +93,42 @@ __device__ __forceinline__ unsigned bk_slot(const Key<NW> &k) {
     return (unsigned)(h >> 40) & (TAB - 1);
 }
 
-template <int NW, int CAP>
+template <int NW, int CAP, int ITEMS>
 __host__ __device__ constexpr size_t bk_smem_bytes() {
-    return (size_t)(2 * CAP) * (2 * NW * 8 + 8 + 1) + (size_t)(4 * CAP) * 4;
+    return (size_t)(BK_THREADS * ITEMS) * (2 * NW * 8 + 8 + 1 + 1) + (size_t)(2 * BK_THREADS * ITEMS) * 4;
 }
 template <int CAP, int ITEMS>
-__host__ __device__ constexpr int bk_threads() { return 2 * CAP / ITEMS; }
-template <int CAP, int ITEMS>
-__host__ __device__ constexpr int bk_min_blocks() {
-    return bk_threads<CAP, ITEMS>() >= 512 ? 2 : bk_threads<CAP, ITEMS>() >= 256 ? 4 : 8;
+__host__ __device__ constexpr int bk_group_max() { return BK_THREADS * ITEMS / CAP; }
+
+// Position in output bucket lb for every lane that passes `want`: lanes of a warp
+// with the same bucket take consecutive slots from one shared-memory atomic.
+__device__ __forceinline__ int bk_claim(int *s_out, int lb, bool want) {
+    const unsigned act = __ballot_sync(0xffffffffu, want);
+    int pos = -1;
+    if (want) {
+        const unsigned peers = __match_any_sync(act, lb);
+        const int leader = __ffs(peers) - 1;
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s_out[lb], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        pos = base + __popc(peers & ((1u << lane) - 1u));
+    }
+    return pos;
 }
 
-// One window-1 rotation: CTA blockIdx.x owns one bucket pair.  k is the
-// rotation's index within the launched group (rotation S->bk_rot0 + k, input
-// set (S->bk_cur0 + k) & 1).
+// One window-1 rotation: CTA blockIdx.x owns bucket pairs
+// [blockIdx.x * group, (blockIdx.x + 1) * group).  k is the rotation's index
+// within the launched group of rotations (rotation S->bk_rot0 + k, input set
+// (S->bk_cur0 + k) & 1).
 template <int NW, int CAP, int ITEMS>
-__global__ void __launch_bounds__(bk_threads<CAP, ITEMS>(), bk_min_blocks<CAP, ITEMS>())
-k_bk_rotate(BkArgs A, int k) {
-    constexpr int THREADS = bk_threads<CAP, ITEMS>();
-    constexpr int MAXT = 2 * CAP;
-    constexpr int TAB = 4 * CAP;
-    static_assert(THREADS * ITEMS == MAXT, "a CTA holds two full buckets");
+__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 : 4) k_bk_rotate(BkArgs A, int k) {
+    constexpr int T = BK_THREADS;
+    constexpr int SMI = T * ITEMS;                 // staged terms
+    constexpr int TAB = 2 * SMI;                   // key index slots
+    constexpr int GMAX = bk_group_max<CAP, ITEMS>();
+    constexpr int NBK = 2 * GMAX;                  // buckets of a group
+    static_assert(GMAX >= 2, "a pair of full buckets fits");
     DevState *S = A.S;
     if (S->err) return;
     const long long r = S->bk_rot0 + k;
@@ -114,18 +136,21 @@ k_bk_rotate(BkArgs A, int k) {
     const int cur = (S->bk_cur0 + k) & 1;
     __shared__ GenRec g;
     __shared__ unsigned s_delta;
-    __shared__ unsigned long long s_scan[THREADS / 32 + 1];
-    __shared__ int s_red[3][THREADS / 32];
+    __shared__ int s_b[NBK], s_n[NBK], s_out[NBK], s_off[NBK + 1];
+    __shared__ int s_j1, s_bad;
+    __shared__ int s_red[3][T / 32];
     extern __shared__ u64 bsm[];
-    u64 *skz = bsm;                                                     // [NW][MAXT]
-    u64 *skx = skz + NW * MAXT;                                         // [NW][MAXT]
-    double *sc = reinterpret_cast<double *>(skx + NW * MAXT);           // [MAXT]
-    unsigned *tab = reinterpret_cast<unsigned *>(sc + MAXT);            // [TAB]
-    unsigned char *sdead = reinterpret_cast<unsigned char *>(tab + TAB);  // [MAXT]
+    u64 *skz = bsm;                                                     // [NW][SMI]
+    u64 *skx = skz + NW * SMI;                                          // [NW][SMI]
+    double *sc = reinterpret_cast<double *>(skx + NW * SMI);            // [SMI]
+    unsigned *tab = reinterpret_cast<unsigned *>(sc + SMI);             // [TAB]
+    unsigned char *sdead = reinterpret_cast<unsigned char *>(tab + TAB);  // [SMI]
+    unsigned char *sbk = sdead + SMI;                                   // [SMI] local bucket of each term
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         g = A.gens[r];
         s_delta = bk_hash<NW>(g.gz, g.gx, A.rows, A.bits);
+        s_bad = 0;
     }
     // the state entering this rotation, from the previous rotation's record (the
     // early-merge rule of spv_evolve.jl:356-362)
@@ -143,171 +168,181 @@ k_bk_rotate(BkArgs A, int k) {
     __syncthreads();
     const unsigned delta = s_delta;
     const int nb = 1 << A.bits;
-    int b0, b1;
-    if (delta == 0) {
-        b0 = 2 * blockIdx.x;
-        b1 = b0 + 1;
-    } else {
-        const int low = __ffs(delta) - 1;
-        const int p = blockIdx.x;
-        b0 = ((p >> low) << (low + 1)) | (p & ((1 << low) - 1));
-        b1 = b0 ^ (int)delta;
-    }
-    if (b0 >= nb || b1 >= nb) {
+    const int G = A.group;
+    if (G < 1 || G > GMAX) {
         if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
         return;
     }
     const int *CNT = A.cnt[cur];
-    const int n0 = CNT[b0], n1 = CNT[b1];
-    if (n0 < 0 || n1 < 0 || n0 > CAP || n1 > CAP) {
+    if (tid < G) {
+        // pair p = blockIdx.x * G + tid: buckets (b0, b0 xor delta), or (2p, 2p + 1) when delta = 0
+        const int p = blockIdx.x * G + tid;
+        int b0, b1;
+        if (delta == 0) {
+            b0 = 2 * p;
+            b1 = b0 + 1;
+        } else {
+            const int low = __ffs(delta) - 1;
+            b0 = ((p >> low) << (low + 1)) | (p & ((1 << low) - 1));
+            b1 = b0 ^ (int)delta;
+        }
+        int n0 = 0, n1 = 0;
+        if (b0 >= nb || b1 >= nb) {
+            s_bad = 1;
+        } else {
+            n0 = CNT[b0];
+            n1 = CNT[b1];
+            if (n0 < 0 || n1 < 0 || n0 > CAP || n1 > CAP) s_bad = 1;
+        }
+        s_b[2 * tid] = b0; s_b[2 * tid + 1] = b1;
+        s_n[2 * tid] = s_bad ? 0 : n0; s_n[2 * tid + 1] = s_bad ? 0 : n1;
+    }
+    if (tid < NBK) s_out[tid] = 0;
+    __syncthreads();
+    if (s_bad) {
         if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
         return;
     }
-    const int ntot = n0 + n1;
     const u64 *Z = A.z[cur], *X = A.x[cur];
     const double *C = A.c[cur];
-    // ---- stage both buckets (item i < n0: bucket b0 slot i, else b1 slot i - n0)
-#pragma unroll
-    for (int it = 0; it < ITEMS; ++it) {
-        const int i = it * THREADS + tid;
-        if (i < ntot) {
-            const long long p = i < n0 ? (long long)b0 * CAP + i : (long long)b1 * CAP + (i - n0);
-            const Key<NW> kk = load_key<NW>(Z, X, p);
-#pragma unroll
-            for (int w = 0; w < NW; ++w) { skz[w * MAXT + i] = kk.z[w]; skx[w * MAXT + i] = kk.x[w]; }
-            sc[i] = C[p];
-        }
-    }
-    for (int s = tid; s < TAB; s += THREADS) tab[s] = 0u;
-    __syncthreads();
+    u64 *OZ = A.z[cur ^ 1], *OX = A.x[cur ^ 1];
+    double *OC = A.c[cur ^ 1];
     const DevParams &P = *A.P;
-    auto skey = [&](int i) {
-        Key<NW> kk;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) { kk.z[w] = skz[w * MAXT + i]; kk.x[w] = skx[w * MAXT + i]; }
-        return kk;
-    };
-    // ---- index the keys; mark the terms the early merge drops
-#pragma unroll
-    for (int it = 0; it < ITEMS; ++it) {
-        const int i = it * THREADS + tid;
-        if (i < ntot) {
-            const Key<NW> kk = skey(i);
-            unsigned s = bk_slot<NW, TAB>(kk);
-            for (int probe = 0; probe < TAB; ++probe) {
-                if (atomicCAS(&tab[s], 0u, (unsigned)(i + 1)) == 0u) break;
-                s = (s + 1) & (TAB - 1);
-            }
-            sdead[i] = (pref && should_drop<NW>(P.strict, kk, fabs(sc[i]))) ? 1 : 0;
-        }
-    }
-    __syncthreads();
-    auto find = [&](const Key<NW> &q) {
-        unsigned s = bk_slot<NW, TAB>(q);
-        for (int probe = 0; probe < TAB; ++probe) {
-            const unsigned e = tab[s];
-            if (e == 0u) return -1;
-            const int j = (int)e - 1;
-            if (key_eq<NW>(skey(j), q)) return j;
-            s = (s + 1) & (TAB - 1);
-        }
-        return -1;
-    };
     const bool do_chan = (g.flags & GEN_CHANNEL) != 0 && P.chan_kind >= 0;
     const bool local_on = P.local_active != 0;
     const double cv = g.cosv, sv = g.sinv;
-    // ---- each thread: items ITEMS * tid + q (contiguous, so its outputs are);
-    // a new term's key is recomputed as key xor M when it is written
-    double oval[ITEMS], nval[ITEMS];
-    unsigned keepm = 0;           // bit q: own output kept; bit 8 + q: new term kept
-    int cre = 0, alive = 0;
-#pragma unroll
-    for (int q = 0; q < ITEMS; ++q) {
-        const int i = ITEMS * tid + q;
-        oval[q] = 0.0;
-        nval[q] = 0.0;
-        if (i >= ntot || sdead[i]) continue;
-        ++alive;
-        const Key<NW> kk = skey(i);
-        const double c = sc[i];
-        double v = c;
-        Key<NW> qk;
-        double sg = 0.0;
-        if (rotate_term<NW>(kk, g, &qk, &sg)) {
-            v = __dmul_rn(c, cv);
-            const double s = __dmul_rn(sg * sv, c);          // (k - 2) * sin(theta) * c, spv_kernels.jl:163
-            const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
-            cre += s_ok ? 1 : 0;
-            const int j = find(qk);
-            if (j >= 0 && !sdead[j]) {
-                // the partner's sin branch lands on this key: live value first, then the append
-                const Key<NW> kj = skey(j);
-                Key<NW> back;
-                double sgj = 0.0;
-                rotate_term<NW>(kj, g, &back, &sgj);
-                const double t = __dmul_rn(sgj * sv, sc[j]);
-                if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
-            } else if (s_ok && !should_drop<NW>(P.strict, qk, fabs(s))) {
-                nval[q] = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
-                keepm |= 1u << (8 + q);
-            }
-        }
-        if (!should_drop<NW>(P.strict, kk, fabs(v))) {
-            oval[q] = do_chan ? __dmul_rn(v, channel_factor<NW>(P, kk)) : v;
-            keepm |= 1u << q;
-        }
-    }
-    // ---- output positions: per output bucket, own survivors (item order) then new terms
-    // packed counters: [15:0] own b0, [31:16] own b1, [47:32] new b0, [63:48] new b1
     const int flip = delta != 0 ? 1 : 0;
-    unsigned long long mine = 0;
+    auto skey = [&](int i) {
+        Key<NW> kk;
 #pragma unroll
-    for (int q = 0; q < ITEMS; ++q) {
-        const int i = ITEMS * tid + q;
-        const int ob = i < n0 ? 0 : 1;
-        if ((keepm >> q) & 1u) mine += 1ull << (16 * ob);
-        if ((keepm >> (8 + q)) & 1u) mine += 1ull << (16 * (2 + (ob ^ flip)));
-    }
-    unsigned long long tot;
-    unsigned long long base = block_excl_scan<THREADS>(mine, 0ull, OpSum(), s_scan, &tot);
-    const int own0 = (int)(tot & 0xffff), own1 = (int)((tot >> 16) & 0xffff);
-    const int cnt0 = own0 + (int)((tot >> 32) & 0xffff), cnt1 = own1 + (int)((tot >> 48) & 0xffff);
-    u64 *OZ = A.z[cur ^ 1], *OX = A.x[cur ^ 1];
-    double *OC = A.c[cur ^ 1];
+        for (int w = 0; w < NW; ++w) { kk.z[w] = skz[w * SMI + i]; kk.x[w] = skx[w * SMI + i]; }
+        return kk;
+    };
+    int cre = 0, alive = 0, kept = 0;
     bool over = false;
+    // ---- sub-groups of consecutive pairs whose terms fit the staging area
+    for (int j0 = 0; j0 < G;) {
+        if (tid == 0) {
+            int j = j0, tot = 0;
+            while (j < G && tot + s_n[2 * j] + s_n[2 * j + 1] <= SMI) {
+                s_off[2 * (j - j0)] = tot;
+                tot += s_n[2 * j];
+                s_off[2 * (j - j0) + 1] = tot;
+                tot += s_n[2 * j + 1];
+                ++j;
+            }
+            s_off[2 * (j - j0)] = tot;
+            s_j1 = j;
+        }
+        __syncthreads();
+        const int j1 = s_j1;
+        const int nloc = 2 * (j1 - j0);            // buckets of this sub-group
+        const int ntot = s_off[nloc];
+        // stage: term i lies in local bucket lb with s_off[lb] <= i < s_off[lb + 1]
+        for (int i = tid; i < ntot; i += T) {
+            int lb = 0;
+            while (lb + 1 < nloc && s_off[lb + 1] <= i) ++lb;
+            const long long p = (long long)s_b[2 * j0 + lb] * CAP + (i - s_off[lb]);
+            const Key<NW> kk = load_key<NW>(Z, X, p);
 #pragma unroll
-    for (int q = 0; q < ITEMS; ++q) {
-        const int i = ITEMS * tid + q;
-        const int ob = i < n0 ? 0 : 1;
-        if ((keepm >> q) & 1u) {
-            const int pos = (int)((base >> (16 * ob)) & 0xffff);
-            base += 1ull << (16 * ob);
-            if (pos < CAP) {
-                const long long o = (long long)(ob ? b1 : b0) * CAP + pos;
-                store_key<NW>(OZ, OX, o, skey(i));
-                OC[o] = oval[q];
-            } else {
-                over = true;
+            for (int w = 0; w < NW; ++w) { skz[w * SMI + i] = kk.z[w]; skx[w * SMI + i] = kk.x[w]; }
+            sc[i] = C[p];
+            sbk[i] = (unsigned char)(2 * j0 + lb);
+        }
+        for (int s2 = tid; s2 < TAB; s2 += T) tab[s2] = 0u;
+        __syncthreads();
+        // index the keys; mark the terms the early merge drops
+        for (int i = tid; i < ntot; i += T) {
+            const Key<NW> kk = skey(i);
+            unsigned h = bk_slot<NW, TAB>(kk);
+            for (int probe = 0; probe < TAB; ++probe) {
+                if (atomicCAS(&tab[h], 0u, (unsigned)(i + 1)) == 0u) break;
+                h = (h + 1) & (TAB - 1);
+            }
+            sdead[i] = (pref && should_drop<NW>(P.strict, kk, fabs(sc[i]))) ? 1 : 0;
+        }
+        __syncthreads();
+        auto find = [&](const Key<NW> &q) {
+            unsigned h = bk_slot<NW, TAB>(q);
+            for (int probe = 0; probe < TAB; ++probe) {
+                const unsigned e = tab[h];
+                if (e == 0u) return -1;
+                const int j = (int)e - 1;
+                if (key_eq<NW>(skey(j), q)) return j;
+                h = (h + 1) & (TAB - 1);
+            }
+            return -1;
+        };
+        // each term: own output (in its bucket) and new sin-branch term (in the partner bucket)
+        const int rounds = (ntot + T - 1) / T;
+        for (int rd = 0; rd < rounds; ++rd) {
+            const int i = rd * T + tid;
+            const bool in = i < ntot && !sdead[i];
+            bool own = false, nw_ = false;
+            double oval = 0.0, nval = 0.0;
+            int lb = 0;
+            if (in) {
+                ++alive;
+                lb = sbk[i];
+                const Key<NW> kk = skey(i);
+                const double c = sc[i];
+                double v = c;
+                Key<NW> qk;
+                double sg = 0.0;
+                if (rotate_term<NW>(kk, g, &qk, &sg)) {
+                    v = __dmul_rn(c, cv);
+                    const double s = __dmul_rn(sg * sv, c);      // (k - 2) * sin(theta) * c, spv_kernels.jl:163
+                    const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
+                    cre += s_ok ? 1 : 0;
+                    const int j = find(qk);
+                    if (j >= 0 && !sdead[j]) {
+                        // the partner's sin branch lands on this key: live value first, then the append
+                        const Key<NW> kj = skey(j);
+                        Key<NW> back;
+                        double sgj = 0.0;
+                        rotate_term<NW>(kj, g, &back, &sgj);
+                        const double t = __dmul_rn(sgj * sv, sc[j]);
+                        if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
+                    } else if (s_ok && !should_drop<NW>(P.strict, qk, fabs(s))) {
+                        nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
+                        nw_ = true;
+                    }
+                }
+                if (!should_drop<NW>(P.strict, kk, fabs(v))) {
+                    oval = do_chan ? __dmul_rn(v, channel_factor<NW>(P, kk)) : v;
+                    own = true;
+                }
+            }
+            kept += (own ? 1 : 0) + (nw_ ? 1 : 0);
+            const int po = bk_claim(s_out, lb, own);
+            if (own) {
+                if (po < CAP) {
+                    const long long o = (long long)s_b[lb] * CAP + po;
+                    store_key<NW>(OZ, OX, o, skey(i));
+                    OC[o] = oval;
+                } else {
+                    over = true;
+                }
+            }
+            const int tb = lb ^ flip;
+            const int pn = bk_claim(s_out, tb, nw_);
+            if (nw_) {
+                if (pn < CAP) {
+                    const long long o = (long long)s_b[tb] * CAP + pn;
+                    Key<NW> nk = skey(i);
+#pragma unroll
+                    for (int w = 0; w < NW; ++w) { nk.z[w] ^= g.gz[w]; nk.x[w] ^= g.gx[w]; }
+                    store_key<NW>(OZ, OX, o, nk);
+                    OC[o] = nval;
+                } else {
+                    over = true;
+                }
             }
         }
-        if ((keepm >> (8 + q)) & 1u) {
-            const int tb = ob ^ flip;
-            const int pos = (tb ? own1 : own0) + (int)((base >> (16 * (2 + tb))) & 0xffff);
-            base += 1ull << (16 * (2 + tb));
-            if (pos < CAP) {
-                const long long o = (long long)(tb ? b1 : b0) * CAP + pos;
-                Key<NW> nk = skey(i);
-#pragma unroll
-                for (int w = 0; w < NW; ++w) { nk.z[w] ^= g.gz[w]; nk.x[w] ^= g.gx[w]; }
-                store_key<NW>(OZ, OX, o, nk);
-                OC[o] = nval[q];
-            } else {
-                over = true;
-            }
-        }
+        __syncthreads();      // the staging area and index are reused by the next sub-group
+        j0 = j1;
     }
     // ---- counts and per-rotation totals
-    int kept = __popc(keepm & 0xffu) + __popc((keepm >> 8) & 0xffu);
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         kept += __shfl_xor_sync(0xffffffffu, kept, d);
@@ -317,18 +352,18 @@ k_bk_rotate(BkArgs A, int k) {
     if (lane == 0) { s_red[0][warp] = kept; s_red[1][warp] = cre; s_red[2][warp] = alive; }
     if (over) atomicOr(&S->err, ERR_OVERFLOW);
     __syncthreads();
+    int *OCNT = A.cnt[cur ^ 1];
+    BkRec &me = A.rec[r + 1];
+    if (tid < 2 * G) OCNT[s_b[tid]] = min(s_out[tid], CAP);
     if (tid == 0) {
-        int kt = 0, ct = 0, at = 0;
-        for (int w = 0; w < THREADS / 32; ++w) { kt += s_red[0][w]; ct += s_red[1][w]; at += s_red[2][w]; }
-        int *OCNT = A.cnt[cur ^ 1];
-        OCNT[b0] = min(cnt0, CAP);
-        OCNT[b1] = min(cnt1, CAP);
-        BkRec &me = A.rec[r + 1];
+        int kt = 0, ct = 0, at = 0, mx = 0;
+        for (int w = 0; w < T / 32; ++w) { kt += s_red[0][w]; ct += s_red[1][w]; at += s_red[2][w]; }
+        for (int b = 0; b < 2 * G; ++b) mx = max(mx, s_out[b]);
         atomicAdd(&me.n_out, (unsigned long long)kt);
         atomicAdd(&me.created, (unsigned long long)ct);
         if (pref) atomicAdd(&me.np, (unsigned long long)at);
-        atomicMax(&me.maxcnt, max(cnt0, cnt1));
-        if (cnt0 > CAP || cnt1 > CAP) {
+        atomicMax(&me.maxcnt, mx);
+        if (mx > CAP) {
             atomicOr(&S->err, ERR_OVERFLOW);
             atomicMin(&S->bk_fail, r);
         }
