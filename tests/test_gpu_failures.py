@@ -25,9 +25,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _gens(rng, N, L):
+    # rotations on 12 qubits: the set grows ~100x at threshold 1e-2 (bounded)
     gens, angs = [], []
     for _ in range(L):
-        i, j = rng.sample(range(N), 2)
+        i, j = rng.sample(range(12), 2)
         gens.append(((1 << i) | (1 << j), 0) if rng.random() < 0.6 else (0, 1 << i))
         angs.append(rng.uniform(0.2, 1.2))
     return gens, angs
@@ -42,9 +43,9 @@ def test_injected_allocation_failure_leaves_handle_usable(after, path):
     keys = sorted(terms)
     z, x = pp.pack_keys(N, keys)
     c = np.array([terms[k] for k in keys])
-    gens, angs = _gens(rng, N, 64)
+    gens, angs = _gens(rng, N, 40)
     G = [pp.PauliBasis(N, a, b) for a, b in gens]
-    spec = ("coeff", 1e-5)
+    spec = ("coeff", 1e-2)
     old = os.environ.get("PAULIPROP_WINDOW1_PATH")
     os.environ["PAULIPROP_WINDOW1_PATH"] = path
     try:
