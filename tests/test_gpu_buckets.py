@@ -29,6 +29,8 @@ VARIANTS = [(128, 4), (256, 4), (256, 8), (512, 8), (512, 16), (1024, 16)]
 
 
 def _gens(rng, N, L):
+    """One- to three-qubit rotations and dense strings (small angles).  With the
+    thresholds used below the live sets stay within a few million terms."""
     gens, angs = [], []
     for _ in range(L):
         q = rng.sample(range(N), 3)
@@ -46,7 +48,7 @@ def _gens(rng, N, L):
         else:
             m = (1 << N) - 1
             gens.append((rng.getrandbits(N) & m, rng.getrandbits(N) & m))     # dense string
-        angs.append(rng.uniform(-1.5, 1.5))
+        angs.append(rng.uniform(0.02, 0.08) if kind == 5 else rng.uniform(-1.2, 1.2))
     return gens, angs
 
 
@@ -85,10 +87,11 @@ def _on(path, fn):
 
 
 @pytest.mark.parametrize("N", [30, 64, 100])
-@pytest.mark.parametrize("spec", [("coeff", 1e-6), ("comp", [("coeff", 1e-7), ("weight", 20)])], ids=str)
+@pytest.mark.parametrize("spec", ["coeff", "comp"])
 def test_bucket_random_sequences(N, spec):
+    spec = ("coeff", 1e-2) if spec == "coeff" else ("comp", [("coeff", 1e-2), ("weight", 3 * N // 4 + 2)])
     rng = random.Random(7 * N)
-    terms = rand_terms(rng, N, 20_000)
+    terms = rand_terms(rng, N, 5000)
     gens, angs = _gens(rng, N, 48)
     v = _oracle(N, terms)
     g = _gpu(v, N)
@@ -116,9 +119,9 @@ def test_bucket_every_variant(variant):
     load divisors and chunks, gives the oracle's vector bit for bit."""
     rng = random.Random(sum(variant))
     for N in (64, 90):
-        terms = rand_terms(rng, N, 8_000)
+        terms = rand_terms(rng, N, 4000)
         gens, angs = _gens(rng, N, 40)
-        spec = ("coeff", 1e-6)
+        spec = ("coeff", 1e-2)
         v = _oracle(N, terms)
         g = _gpu(v, N, tuning=(variant[0], variant[1], 3, 8))
         tn = _lib.PPTuning()
@@ -142,11 +145,11 @@ def test_bucket_early_merge_prefilter():
     come back as new sin branches of their live partners)."""
     rng = random.Random(11)
     N = 40
-    terms = rand_terms(rng, N, 12_000)
-    for k in list(terms)[:4000]:
-        terms[k] = 1e-9 * (rng.random() - 0.5)       # below the threshold before any rotation
+    terms = rand_terms(rng, N, 6000)
+    for k in list(terms)[:2000]:
+        terms[k] = 1e-3 * (rng.random() - 0.5)       # below the threshold before any rotation
     gens, angs = _gens(rng, N, 40)
-    spec = ("coeff", 1e-6)
+    spec = ("coeff", 1e-2)
     v = _oracle(N, terms, append_factor=0.05, min_capacity=4)
     g = _gpu(v, N)
     _, ctr = v.evolve(gens, angs, window=1, strict=filt(spec), nwin=len(gens))
@@ -163,9 +166,9 @@ def test_bucket_early_merge_prefilter():
 @pytest.mark.parametrize("N", [50, 90])
 def test_bucket_local_truncation_and_channel(N):
     rng = random.Random(3 + N)
-    terms = rand_terms(rng, N, 15_000)
+    terms = rand_terms(rng, N, 5000)
     gens, angs = _gens(rng, N, 36)
-    spec, lspec = ("comp", [("coeff", 1e-6), ("weight", 3 * N // 4 + 4)]), ("coeff", 2e-4)
+    spec, lspec = ("comp", [("coeff", 1e-2), ("weight", 3 * N // 4 + 4)]), ("coeff", 2e-2)
     per = 12
     v = _oracle(N, terms)
     g = _gpu(v, N)
