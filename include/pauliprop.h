@@ -300,13 +300,13 @@ const char *pp_last_error(void);
 
 /* Launch configuration of the bucketed window-1 rotations (no counterpart in the
  * reference; results do not depend on it).  (bucket_cap, items_per_thread) must be
- * a compiled variant: (128, 4), (256, 4), (256, 8), (512, 8), (512, 16) or
- * (1024, 16); a CTA of 256 threads stages up to 256 * items_per_thread terms of a
- * group of bucket pairs.  load_div (3..16): bucketing aims at a mean load of at
+ * a compiled variant: (128, 4), (256, 4), (512, 4), (256, 8), (512, 8) or
+ * (1024, 8); a CTA of 256 threads has two staging areas of 256 * items_per_thread
+ * terms (a group of bucket pairs in one, the next group's terms in the other).  load_div (3..16): bucketing aims at a mean load of at
  * most bucket_cap / load_div.  chunk (8..256): rotations launched between host
  * checks.  pauliprop's autotuner (pauliprop/tune.py) measures the variants on the
  * device and caches the fastest per (word count, SM count); a new handle starts
- * with (256, 8, 5, 64). */
+ * with (256, 4, 5, 64). */
 typedef struct {
     int32_t bucket_cap, items_per_thread, load_div, chunk;
 } pp_tuning;

@@ -125,6 +125,7 @@ struct pp_spv {
     std::unordered_map<int, cudaGraphExec_t> bk_graphs;   // key: bits * 4 + chunk class
     long long bk_graph_gen = -1;
     pp_tuning tune = {BK_DEFAULT_CAP, BK_DEFAULT_ITEMS, 5, 64};   // pp_set_tuning
+    struct { int occ1 = 1, occ2 = 1; } bk_occ[8];                  // resident CTAs per SM of each variant
 };
 
 // ------------------------------------------------------------------ helpers
@@ -370,7 +371,12 @@ static int ensure_append(pp_spv *h, long long need, long long pending) {
 }
 
 static int check_err(pp_spv *h, const DevState &st) {
-    if (st.err & ERR_BOUNDS) return fail(PP_DEVICE_ERROR, "internal error: a computed index fell outside its buffer");
+    if (st.err & ERR_BOUNDS) {
+        char b[160];
+        snprintf(b, sizeof b, "internal error: a computed index fell outside its buffer (check %llu, value %llu)",
+                 st.dbg >> 40, st.dbg & 0xffffffffffull);
+        return fail(PP_DEVICE_ERROR, b);
+    }
     if (st.err & ERR_TIMEOUT) return fail(PP_TIMEOUT, "a device-side look-back wait timed out");
     if (st.err & ERR_TILE) return fail(PP_ERROR_EXCEPTION, "an equal-key run exceeded the merge tile staging size");
     return PP_OK;
@@ -825,11 +831,13 @@ struct BkVariant {
     BkKernel k1, k2;
     size_t smem1, smem2;
 };
+
 #define PP_BK_VARIANT(C, I)                                                                                 \
     { C, I, bk_group_max<C, I>(), k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, bk_smem_bytes<1, C, I>(),     \
       bk_smem_bytes<2, C, I>() }
-static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(128, 4), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(256, 8),
-                                        PP_BK_VARIANT(512, 8), PP_BK_VARIANT(512, 16), PP_BK_VARIANT(1024, 16)};
+static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(128, 4), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(512, 4),
+                                        PP_BK_VARIANT(256, 8), PP_BK_VARIANT(512, 8), PP_BK_VARIANT(1024, 8)};
+static constexpr int BK_NVAR = sizeof(BK_VARIANTS) / sizeof(BK_VARIANTS[0]);
 #undef PP_BK_VARIANT
 
 static const BkVariant *bk_variant(int cap, int items) {
@@ -838,18 +846,22 @@ static const BkVariant *bk_variant(int cap, int items) {
     return nullptr;
 }
 
-// Bucket pairs per CTA for 2^bits buckets: as many as the variant stages, but
-// small enough to give every SM a few CTAs.
+// Bucket pairs per group for 2^bits buckets: about 0.6 of a staging area at the
+// typical load (a bucket averages about cap / 3.5 terms between splits), but
+// small enough that every resident CTA gets groups.
 static int bk_group_for(pp_spv *h, const BkVariant *v, int bits) {
     const long long pairs = 1ll << (bits - 1);
+    const int want = std::max(1, (int)(1.05 * BK_THREADS * v->items / v->cap));
     int gsz = 1;
-    while (gsz * 2 <= v->gmax && pairs / (gsz * 2) >= 4ll * h->nsm) gsz *= 2;
+    while (gsz * 2 <= std::min(want, v->gmax) && pairs / (gsz * 2) >= 2ll * h->nsm) gsz *= 2;
     return gsz;
 }
 
 template <int NW>
 static void bk_launch(pp_spv *h, const BkVariant *v, const BkArgs &A, int k) {
-    const int grid = (int)((1ll << (A.bits - 1)) / A.group);
+    const long long groups = (1ll << (A.bits - 1)) / A.group;
+    const int occ = NW == 1 ? h->bk_occ[v - BK_VARIANTS].occ1 : h->bk_occ[v - BK_VARIANTS].occ2;
+    const int grid = (int)std::min(groups, (long long)h->nsm * occ);
     (NW == 1 ? v->k1 : v->k2)<<<grid, BK_THREADS, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
 }
 
@@ -874,9 +886,17 @@ static int bk_rows_init(pp_spv *h) {
     h->bk_rows = dr;
     h->bk_aux = da;
     CU(cudaMemcpyAsync(h->bk_rows, rows, sizeof rows, cudaMemcpyHostToDevice, h->stream));
-    for (const BkVariant &v : BK_VARIANTS) {
+    for (int i = 0; i < BK_NVAR; ++i) {
+        const BkVariant &v = BK_VARIANTS[i];
         CU(cudaFuncSetAttribute(v.k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem1));
         CU(cudaFuncSetAttribute(v.k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem2));
+        CU(cudaFuncSetAttribute(v.k1, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+        CU(cudaFuncSetAttribute(v.k2, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+        int o = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, v.k1, BK_THREADS, v.smem1));
+        h->bk_occ[i].occ1 = std::max(1, o);
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, v.k2, BK_THREADS, v.smem2));
+        h->bk_occ[i].occ2 = std::max(1, o);
     }
     return sync_check(h);
 }
@@ -893,6 +913,8 @@ static BkArgs bk_args(pp_spv *h, const BkVariant *v, int bits, BkRec *rec) {
     memset(&A, 0, sizeof A);
     for (int s = 0; s < 2; ++s) { A.z[s] = h->bkz[s]; A.x[s] = h->bkx[s]; A.c[s] = h->bkc[s]; A.cnt[s] = h->bkcnt[s]; }
     A.bits = bits;
+    A.bits_cap = h->bk_bits_cap;
+    A.rec_len = h->bk_rec_cap;
     A.group = bk_group_for(h, v, bits);
     A.rows = h->bk_rows;
     A.rec = rec;
@@ -1042,7 +1064,8 @@ static int bk_to_dense(pp_spv *h, int cur, int bits) {
     TRY(radix_reserve(h, n));
     TRY(ensure_live(h, n + 1, false));
     k_bk_gather<NW><<<std::max(1, std::min(h->nsm * 8, (nb + 7) / 8)), 256, 0, s>>>(
-        h->bkz[cur], h->bkx[cur], h->bkc[cur], h->bkcnt[cur], nb, h->bk_cap, h->bk_off, h->z[0], h->x[0], h->c[0]);
+        h->bkz[cur], h->bkx[cur], h->bkc[cur], h->bkcnt[cur], nb, h->bk_cap, h->bk_off, h->z[0], h->x[0], h->c[0],
+        h->cap, h->S);
     TRY(sync_check(h));
     int in_t = 0;
     TRY(radix_sort<NW>(h, h->z[0], h->x[0], h->c[0], h->z[1], h->x[1], h->c[1], n, &in_t));
@@ -1094,6 +1117,8 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
     const int chunk = h->tune.chunk;
     while (done < L) {
         const long long len = std::min((long long)chunk, L - done);
+        if (bits < 1 || bits > h->bk_bits_cap || h->bk_cap != var->cap || L + 1 > h->bk_rec_cap || (cur & ~1))
+            return fail(PP_ERROR_EXCEPTION, "internal error: inconsistent bucket layout before a launch");
         k_bk_begin<<<1, 1, 0, s>>>(h->S, done, cur, 1);
         prof->launches += 1;
         if (!timed) {
@@ -1933,7 +1958,7 @@ extern "C" int pp_set_tuning(pp_spv *h, const pp_tuning *t) {
     if (!h || !t) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: null argument");
     if (!bk_variant(t->bucket_cap, t->items_per_thread))
         return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: (bucket_cap, items_per_thread) must be one of (128, 4), "
-                                       "(256, 4), (256, 8), (512, 8), (512, 16), (1024, 16)");
+                                       "(256, 4), (512, 4), (256, 8), (512, 8), (1024, 8)");
     if (t->load_div < 3 || t->load_div > 16) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: load_div must be in 3..16");
     if (t->chunk < 8 || t->chunk > 256) return fail(PP_ARGUMENT_ERROR, "pp_set_tuning: chunk must be in 8..256");
     if (t->bucket_cap != h->tune.bucket_cap || t->items_per_thread != h->tune.items_per_thread ||

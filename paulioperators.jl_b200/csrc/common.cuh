@@ -92,7 +92,15 @@ struct DevState {
     long long bk_fail;            // bucketed rotations: first rotation whose output overflowed a bucket
     int bk_cur0;                  // bucketed rotations: input bucket set of the group's first rotation
     int bk_pad;
+    unsigned long long dbg;       // first failed device check: site << 40 | value (0: none)
 };
+
+// Records a failed device-side check (the access it guards is skipped): the
+// error bit ERR_BOUNDS and, for the first failure only, which check and value.
+__device__ __forceinline__ void flag_bounds(DevState *S, int site, long long value) {
+    atomicOr(&S->err, ERR_BOUNDS);
+    atomicCAS(&S->dbg, 0ull, ((unsigned long long)site << 40) | ((unsigned long long)value & 0xffffffffffull));
+}
 
 // Static per-kernel configuration.
 constexpr int A_THREADS = 512;

@@ -14,13 +14,14 @@
 // pseudo-random rows R_r.  Linearity gives h(P xor M) = h(P) xor h(M), so for
 // the rotation's generator the partner of every term of bucket b lies in bucket
 // b xor delta, delta = h(M), and the sin branch of a term of b belongs to
-// b xor delta as well.  A CTA therefore owns whole bucket pairs {b, b xor delta}
-// (two neighbouring buckets when delta = 0): it loads a group of pairs into
-// shared memory, indexes their keys in a shared-memory hash table, finds each
-// anticommuting term's partner there, and appends each output term to its
-// bucket of the other bucket set (positions from shared-memory counters, so the
-// order inside a bucket is arbitrary; nothing depends on it).  No cross-CTA
-// scan, sort or wait is involved.
+// b xor delta as well.  A CTA therefore works on whole bucket pairs
+// {b, b xor delta} (two neighbouring buckets when delta = 0): it stages a group
+// of pairs in shared memory, indexes their keys in a shared-memory hash table,
+// finds each anticommuting term's partner there, and appends each output term
+// to its bucket of the other bucket set (positions from shared-memory counters,
+// so the order inside a bucket is arbitrary; nothing depends on it).  The grid
+// is persistent and the next group's terms are copied in (cp.async) while a
+// group is processed.  No cross-CTA scan, sort or wait is involved.
 //
 // Per rotation, per term: the early-merge pre-filter, the cos branch, the sum
 // with the partner's sin branch (or a new term when the partner is absent or was
@@ -34,15 +35,13 @@
 namespace pp {
 
 // Compiled (bucket capacity, items per thread) variants; the autotuner picks
-// one per device.  A CTA of BK_THREADS threads stages up to BK_THREADS * ITEMS
-// terms: a group of up to that many / CAP bucket pairs, processed in one pass
-// when their terms fit (else in consecutive sub-groups; a single pair always
-// fits, 2 * CAP <= BK_THREADS * ITEMS), with a shared-memory key index of twice
-// as many slots.
+// one per device.  A CTA of BK_THREADS threads has two staging areas of
+// BK_THREADS * ITEMS terms: one holds the group of bucket pairs being processed,
+// the other receives the next group's terms in the meantime.
 constexpr int BK_ROWS = 26;                    // hash rows: at most 2^26 buckets
 constexpr int BK_THREADS = 256;
 constexpr int BK_DEFAULT_CAP = 256;
-constexpr int BK_DEFAULT_ITEMS = 8;
+constexpr int BK_DEFAULT_ITEMS = 4;
 
 // Per-rotation record: rec[r] describes the live set entering rotation r (the
 // output of rotation r - 1); rotation r reads it and fills rec[r + 1].
@@ -61,6 +60,8 @@ struct BkArgs {
     double *c[2];
     int *cnt[2];                    // terms per bucket
     int bits;                       // 2^bits buckets
+    int bits_cap;                   // the bucket sets and counts are allocated for 2^bits_cap buckets
+    long long rec_len;              // entries of rec
     int group;                      // bucket pairs per CTA (a power of two)
     const u64 *rows;                // [BK_ROWS][4]: z words 0..1, x words 0..1 of each hash row
     BkRec *rec;
@@ -93,12 +94,27 @@ __device__ __forceinline__ unsigned bk_slot(const Key<NW> &k) {
     return (unsigned)(h >> 40) & (TAB - 1);
 }
 
+// Shared memory of k_bk_rotate: two staging areas (keys, coefficients, local
+// bucket of each term), the key index and the pre-filter flags.
 template <int NW, int CAP, int ITEMS>
 __host__ __device__ constexpr size_t bk_smem_bytes() {
-    return (size_t)(BK_THREADS * ITEMS) * (2 * NW * 8 + 8 + 1 + 1) + (size_t)(2 * BK_THREADS * ITEMS) * 4;
+    return (size_t)(BK_THREADS * ITEMS) * (2 * (2 * NW * 8 + 8 + 1) + 2 * 4 + 1);
 }
+// Bucket pairs a group may hold: the host picks a power of two up to this.
 template <int CAP, int ITEMS>
-__host__ __device__ constexpr int bk_group_max() { return BK_THREADS * ITEMS / CAP; }
+__host__ __device__ constexpr int bk_group_max() { return 2 * BK_THREADS * ITEMS / CAP; }
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Position in output bucket lb for every lane that passes `want`: lanes of a warp
 // with the same bucket take consecutive slots from one shared-memory atomic.
@@ -117,18 +133,35 @@ __device__ __forceinline__ int bk_claim(int *s_out, int lb, bool want) {
     return pos;
 }
 
-// One window-1 rotation: CTA blockIdx.x owns bucket pairs
-// [blockIdx.x * group, (blockIdx.x + 1) * group).  k is the rotation's index
-// within the launched group of rotations (rotation S->bk_rot0 + k, input set
+// Buckets of pair p: (b0, b0 xor delta), or (2p, 2p + 1) when delta = 0.
+__device__ __forceinline__ void bk_pair(unsigned delta, long long p, int *b0, int *b1) {
+    if (delta == 0) {
+        *b0 = (int)(2 * p);
+        *b1 = *b0 + 1;
+    } else {
+        const int low = __ffs(delta) - 1;
+        *b0 = (int)(((p >> low) << (low + 1)) | (p & ((1ll << low) - 1)));
+        *b1 = *b0 ^ (int)delta;
+    }
+}
+
+// One window-1 rotation.  The grid is persistent: CTA c processes the groups
+// c, c + gridDim.x, ... of `group` consecutive bucket pairs, and while it
+// processes one group its copies of the next group's terms are in flight
+// (cp.async into the other staging area).  A group whose terms exceed the
+// staging area is processed in sub-groups of consecutive pairs, loaded in turn
+// (a single pair always fits: 2 * CAP <= BK_THREADS * ITEMS).  k is the
+// rotation's index within the launched graph (rotation S->bk_rot0 + k, input set
 // (S->bk_cur0 + k) & 1).
 template <int NW, int CAP, int ITEMS>
-__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 : 4) k_bk_rotate(BkArgs A, int k) {
+__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(BkArgs A, int k) {
     constexpr int T = BK_THREADS;
-    constexpr int SMI = T * ITEMS;                 // staged terms
+    constexpr int SMI = T * ITEMS;                 // staged terms per area
     constexpr int TAB = 2 * SMI;                   // key index slots
     constexpr int GMAX = bk_group_max<CAP, ITEMS>();
     constexpr int NBK = 2 * GMAX;                  // buckets of a group
-    static_assert(GMAX >= 2, "a pair of full buckets fits");
+    static_assert(2 * CAP <= SMI, "a pair of full buckets fits");
+    static_assert(NBK <= 256, "local bucket index fits a byte");
     DevState *S = A.S;
     if (S->err) return;
     const long long r = S->bk_rot0 + k;
@@ -136,21 +169,32 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
     const int cur = (S->bk_cur0 + k) & 1;
     __shared__ GenRec g;
     __shared__ unsigned s_delta;
-    __shared__ int s_b[NBK], s_n[NBK], s_out[NBK], s_off[NBK + 1];
-    __shared__ int s_j1, s_bad;
+    __shared__ int s_b[2][NBK], s_n[2][NBK], s_off[2][NBK + 1], s_j1[2];
+    __shared__ int s_out[NBK], s_mx, s_bad;
     __shared__ int s_red[3][T / 32];
     extern __shared__ u64 bsm[];
-    u64 *skz = bsm;                                                     // [NW][SMI]
-    u64 *skx = skz + NW * SMI;                                          // [NW][SMI]
-    double *sc = reinterpret_cast<double *>(skx + NW * SMI);            // [SMI]
-    unsigned *tab = reinterpret_cast<unsigned *>(sc + SMI);             // [TAB]
-    unsigned char *sdead = reinterpret_cast<unsigned char *>(tab + TAB);  // [SMI]
-    unsigned char *sbk = sdead + SMI;                                   // [SMI] local bucket of each term
+    // staging area a: keys (NW words each, z then x), coefficients, local buckets
+    u64 *skz[2], *skx[2];
+    double *sc[2];
+    skz[0] = bsm;
+    skx[0] = skz[0] + NW * SMI;
+    sc[0] = reinterpret_cast<double *>(skx[0] + NW * SMI);
+    skz[1] = reinterpret_cast<u64 *>(sc[0] + SMI);
+    skx[1] = skz[1] + NW * SMI;
+    sc[1] = reinterpret_cast<double *>(skx[1] + NW * SMI);
+    unsigned *tab = reinterpret_cast<unsigned *>(sc[1] + SMI);           // [TAB]
+    unsigned char *sbk0 = reinterpret_cast<unsigned char *>(tab + TAB);  // [2][SMI]
+    unsigned char *sdead = sbk0 + 2 * SMI;                               // [SMI]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         g = A.gens[r];
         s_delta = bk_hash<NW>(g.gz, g.gx, A.rows, A.bits);
         s_bad = 0;
+        s_mx = 0;
+    }
+    if (r + 1 >= A.rec_len) {
+        if (tid == 0) flag_bounds(S, 2, r);
+        return;
     }
     // the state entering this rotation, from the previous rotation's record (the
     // early-merge rule of spv_evolve.jl:356-362)
@@ -165,44 +209,18 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
         me.acap = acap;
         me.pref = pref ? 1 : 0;
     }
+    for (int i = tid; i < TAB; i += T) tab[i] = 0u;
+    if (tid < NBK) s_out[tid] = 0;
     __syncthreads();
     const unsigned delta = s_delta;
-    const int nb = 1 << A.bits;
+    const long long nb = 1ll << A.bits;
     const int G = A.group;
-    if (G < 1 || G > GMAX) {
-        if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
+    const long long ngroups = (nb / 2) / G;
+    if (G < 1 || G > GMAX || (nb / 2) % G != 0 || A.bits > A.bits_cap || A.bits < 1) {
+        if (tid == 0) flag_bounds(S, 1, ((long long)A.bits << 16) | G);
         return;
     }
     const int *CNT = A.cnt[cur];
-    if (tid < G) {
-        // pair p = blockIdx.x * G + tid: buckets (b0, b0 xor delta), or (2p, 2p + 1) when delta = 0
-        const int p = blockIdx.x * G + tid;
-        int b0, b1;
-        if (delta == 0) {
-            b0 = 2 * p;
-            b1 = b0 + 1;
-        } else {
-            const int low = __ffs(delta) - 1;
-            b0 = ((p >> low) << (low + 1)) | (p & ((1 << low) - 1));
-            b1 = b0 ^ (int)delta;
-        }
-        int n0 = 0, n1 = 0;
-        if (b0 >= nb || b1 >= nb) {
-            s_bad = 1;
-        } else {
-            n0 = CNT[b0];
-            n1 = CNT[b1];
-            if (n0 < 0 || n1 < 0 || n0 > CAP || n1 > CAP) s_bad = 1;
-        }
-        s_b[2 * tid] = b0; s_b[2 * tid + 1] = b1;
-        s_n[2 * tid] = s_bad ? 0 : n0; s_n[2 * tid + 1] = s_bad ? 0 : n1;
-    }
-    if (tid < NBK) s_out[tid] = 0;
-    __syncthreads();
-    if (s_bad) {
-        if (tid == 0) atomicOr(&S->err, ERR_BOUNDS);
-        return;
-    }
     const u64 *Z = A.z[cur], *X = A.x[cur];
     const double *C = A.c[cur];
     u64 *OZ = A.z[cur ^ 1], *OX = A.x[cur ^ 1];
@@ -212,54 +230,97 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
     const bool local_on = P.local_active != 0;
     const double cv = g.cosv, sv = g.sinv;
     const int flip = delta != 0 ? 1 : 0;
-    auto skey = [&](int i) {
-        Key<NW> kk;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) { kk.z[w] = skz[w * SMI + i]; kk.x[w] = skx[w * SMI + i]; }
-        return kk;
+
+    // pair buckets and counts of group gi into area a (threads < G); -1 group: none
+    auto load_info = [&](int a, long long gi) {
+        if (tid < G) {
+            int b0 = 0, b1 = 0, n0 = 0, n1 = 0;
+            if (gi >= 0) {
+                bk_pair(delta, gi * G + tid, &b0, &b1);
+                if (b0 < 0 || b1 < 0 || b0 >= nb || b1 >= nb) { flag_bounds(S, 3, b0); s_bad = 1; b0 = b1 = 0; }
+                else {
+                    n0 = CNT[b0];
+                    n1 = CNT[b1];
+                    if (n0 < 0 || n1 < 0 || n0 > CAP || n1 > CAP) {
+                        flag_bounds(S, 4, ((long long)n0 << 20) | (n1 & 0xfffff));
+                        s_bad = 1;
+                        n0 = n1 = 0;
+                    }
+                }
+            }
+            s_b[a][2 * tid] = b0; s_b[a][2 * tid + 1] = b1;
+            s_n[a][2 * tid] = n0; s_n[a][2 * tid + 1] = n1;
+        }
+    };
+    // first sub-group [j0, j1) of pairs from j0 that fits the staging area; offsets (thread 0)
+    auto plan = [&](int a, int j0) {
+        if (tid == 0) {
+            int j = j0, tot = 0;
+            while (j < G && tot + s_n[a][2 * j] + s_n[a][2 * j + 1] <= SMI) {
+                s_off[a][2 * (j - j0)] = tot;
+                tot += s_n[a][2 * j];
+                s_off[a][2 * (j - j0) + 1] = tot;
+                tot += s_n[a][2 * j + 1];
+                ++j;
+            }
+            s_off[a][2 * (j - j0)] = tot;
+            s_j1[a] = j;
+        }
+    };
+    // copies of the planned sub-group's terms into area a (asynchronous)
+    auto issue = [&](int a, int j0) {
+        const int nloc = 2 * (s_j1[a] - j0);
+        const int ntot = s_off[a][nloc];
+        unsigned char *sbk = sbk0 + a * SMI;
+        if (ntot > SMI || nloc > NBK) {      // the planner never builds such a sub-group
+            if (tid == 0) flag_bounds(S, 5, ((long long)ntot << 16) | nloc);
+            return;
+        }
+        for (int i = tid; i < ntot; i += T) {
+            int lb = 0;
+            while (lb + 1 < nloc && s_off[a][lb + 1] <= i) ++lb;
+            const int bq = s_b[a][2 * j0 + lb];
+            const long long p = (long long)bq * CAP + (i - s_off[a][lb]);
+            if (bq < 0 || bq >= nb || i - s_off[a][lb] >= CAP) {
+                flag_bounds(S, 6, p);
+                sbk[i] = 0;
+                continue;
+            }
+            if constexpr (NW == 1) {
+                cp_async8(skz[a] + i, Z + p);
+                cp_async8(skx[a] + i, X + p);
+            } else {
+                cp_async16(skz[a] + 2 * i, Z + 2 * p);
+                cp_async16(skx[a] + 2 * i, X + 2 * p);
+            }
+            cp_async8(sc[a] + i, C + p);
+            sbk[i] = (unsigned char)(2 * j0 + lb);
+        }
     };
     int cre = 0, alive = 0, kept = 0;
     bool over = false;
-    // ---- sub-groups of consecutive pairs whose terms fit the staging area
-    for (int j0 = 0; j0 < G;) {
-        if (tid == 0) {
-            int j = j0, tot = 0;
-            while (j < G && tot + s_n[2 * j] + s_n[2 * j + 1] <= SMI) {
-                s_off[2 * (j - j0)] = tot;
-                tot += s_n[2 * j];
-                s_off[2 * (j - j0) + 1] = tot;
-                tot += s_n[2 * j + 1];
-                ++j;
-            }
-            s_off[2 * (j - j0)] = tot;
-            s_j1 = j;
-        }
-        __syncthreads();
-        const int j1 = s_j1;
-        const int nloc = 2 * (j1 - j0);            // buckets of this sub-group
-        const int ntot = s_off[nloc];
-        // stage: term i lies in local bucket lb with s_off[lb] <= i < s_off[lb + 1]
-        for (int i = tid; i < ntot; i += T) {
-            int lb = 0;
-            while (lb + 1 < nloc && s_off[lb + 1] <= i) ++lb;
-            const long long p = (long long)s_b[2 * j0 + lb] * CAP + (i - s_off[lb]);
-            const Key<NW> kk = load_key<NW>(Z, X, p);
+    auto skey = [&](int a, int i) {
+        Key<NW> kk;
 #pragma unroll
-            for (int w = 0; w < NW; ++w) { skz[w * SMI + i] = kk.z[w]; skx[w * SMI + i] = kk.x[w]; }
-            sc[i] = C[p];
-            sbk[i] = (unsigned char)(2 * j0 + lb);
+        for (int w = 0; w < NW; ++w) { kk.z[w] = skz[a][NW * i + w]; kk.x[w] = skx[a][NW * i + w]; }
+        return kk;
+    };
+    // process the staged sub-group of area a (ntot terms); leaves the index clear
+    auto run = [&](int a, int ntot) {
+        const unsigned char *sbk = sbk0 + a * SMI;
+        if (ntot > SMI) {                    // uniform: skipped by every thread (flagged in issue)
+            __syncthreads();
+            return;
         }
-        for (int s2 = tid; s2 < TAB; s2 += T) tab[s2] = 0u;
-        __syncthreads();
         // index the keys; mark the terms the early merge drops
         for (int i = tid; i < ntot; i += T) {
-            const Key<NW> kk = skey(i);
+            const Key<NW> kk = skey(a, i);
             unsigned h = bk_slot<NW, TAB>(kk);
             for (int probe = 0; probe < TAB; ++probe) {
                 if (atomicCAS(&tab[h], 0u, (unsigned)(i + 1)) == 0u) break;
                 h = (h + 1) & (TAB - 1);
             }
-            sdead[i] = (pref && should_drop<NW>(P.strict, kk, fabs(sc[i]))) ? 1 : 0;
+            sdead[i] = (pref && should_drop<NW>(P.strict, kk, fabs(sc[a][i]))) ? 1 : 0;
         }
         __syncthreads();
         auto find = [&](const Key<NW> &q) {
@@ -268,12 +329,11 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
                 const unsigned e = tab[h];
                 if (e == 0u) return -1;
                 const int j = (int)e - 1;
-                if (key_eq<NW>(skey(j), q)) return j;
+                if (key_eq<NW>(skey(a, j), q)) return j;
                 h = (h + 1) & (TAB - 1);
             }
             return -1;
         };
-        // each term: own output (in its bucket) and new sin-branch term (in the partner bucket)
         const int rounds = (ntot + T - 1) / T;
         for (int rd = 0; rd < rounds; ++rd) {
             const int i = rd * T + tid;
@@ -284,8 +344,12 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
             if (in) {
                 ++alive;
                 lb = sbk[i];
-                const Key<NW> kk = skey(i);
-                const double c = sc[i];
+                if (lb >= 2 * G) {
+                    flag_bounds(S, 7, lb);
+                    lb = 0;
+                }
+                const Key<NW> kk = skey(a, i);
+                const double c = sc[a][i];
                 double v = c;
                 Key<NW> qk;
                 double sg = 0.0;
@@ -295,13 +359,14 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
                     const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
                     cre += s_ok ? 1 : 0;
                     const int j = find(qk);
-                    if (j >= 0 && !sdead[j]) {
+                    if (j >= ntot) flag_bounds(S, 8, j);
+                    if (j >= 0 && j < ntot && !sdead[j]) {
                         // the partner's sin branch lands on this key: live value first, then the append
-                        const Key<NW> kj = skey(j);
+                        const Key<NW> kj = skey(a, j);
                         Key<NW> back;
                         double sgj = 0.0;
                         rotate_term<NW>(kj, g, &back, &sgj);
-                        const double t = __dmul_rn(sgj * sv, sc[j]);
+                        const double t = __dmul_rn(sgj * sv, sc[a][j]);
                         if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
                     } else if (s_ok && !should_drop<NW>(P.strict, qk, fabs(s))) {
                         nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
@@ -317,8 +382,8 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
             const int po = bk_claim(s_out, lb, own);
             if (own) {
                 if (po < CAP) {
-                    const long long o = (long long)s_b[lb] * CAP + po;
-                    store_key<NW>(OZ, OX, o, skey(i));
+                    const long long o = (long long)s_b[a][lb] * CAP + po;
+                    store_key<NW>(OZ, OX, o, skey(a, i));
                     OC[o] = oval;
                 } else {
                     over = true;
@@ -328,8 +393,8 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
             const int pn = bk_claim(s_out, tb, nw_);
             if (nw_) {
                 if (pn < CAP) {
-                    const long long o = (long long)s_b[tb] * CAP + pn;
-                    Key<NW> nk = skey(i);
+                    const long long o = (long long)s_b[a][tb] * CAP + pn;
+                    Key<NW> nk = skey(a, i);
 #pragma unroll
                     for (int w = 0; w < NW; ++w) { nk.z[w] ^= g.gz[w]; nk.x[w] ^= g.gx[w]; }
                     store_key<NW>(OZ, OX, o, nk);
@@ -339,10 +404,79 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
                 }
             }
         }
-        __syncthreads();      // the staging area and index are reused by the next sub-group
-        j0 = j1;
+        __syncthreads();
+        for (int i = tid; i < TAB; i += T) tab[i] = 0u;     // for the next sub-group
+    };
+
+    // ---- prologue: group c in area 0 (copies in flight), group c + grid planned in area 1
+    long long gi = blockIdx.x;
+    load_info(0, gi < ngroups ? gi : -1);
+    __syncthreads();
+    plan(0, 0);
+    __syncthreads();
+    issue(0, 0);
+    cp_async_commit();
+    {
+        const long long g1 = gi + gridDim.x;
+        load_info(1, g1 < ngroups ? g1 : -1);
+        __syncthreads();
+        plan(1, 0);
+        __syncthreads();
     }
-    // ---- counts and per-rotation totals
+    for (int it = 0; gi < ngroups; ++it, gi += gridDim.x) {
+        const int a = it & 1;
+        const long long gnext = gi + gridDim.x, gafter = gi + 2 * (long long)gridDim.x;
+        // next group's copies (planned last iteration) go in flight now
+        if (gnext < ngroups) issue(a ^ 1, 0);
+        cp_async_commit();
+        // the group after next: its pair counts load while this group is processed
+        int pb0 = 0, pb1 = 0, pn0 = 0, pn1 = 0;
+        if (tid < G && gafter < ngroups) {
+            bk_pair(delta, gafter * G + tid, &pb0, &pb1);
+            if (pb0 < nb && pb1 < nb) { pn0 = CNT[pb0]; pn1 = CNT[pb1]; }
+        }
+        cp_async_wait<1>();
+        __syncthreads();
+        // this group: its first sub-group is staged in area a, later ones are loaded in turn
+        int j0 = 0;
+        for (;;) {
+            run(a, s_off[a][2 * (s_j1[a] - j0)]);
+            j0 = s_j1[a];
+            if (j0 >= G) break;
+            __syncthreads();
+            plan(a, j0);
+            __syncthreads();
+            issue(a, j0);
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+        }
+        // output counts of the group's buckets
+        if (tid < 2 * G) {
+            const int m = s_out[tid];
+            A.cnt[cur ^ 1][s_b[a][tid]] = min(m, CAP);
+            atomicMax(&s_mx, m);
+            s_out[tid] = 0;
+        }
+        __syncthreads();
+        // area a now takes the group after next
+        if (tid < G) {
+            if (gafter < ngroups) {
+                if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
+                    flag_bounds(S, 10, ((long long)pn0 << 20) | (pn1 & 0xfffff));
+                    s_bad = 1;
+                    pb0 = pb1 = pn0 = pn1 = 0;
+                }
+            }
+            s_b[a][2 * tid] = pb0; s_b[a][2 * tid + 1] = pb1;
+            s_n[a][2 * tid] = pn0; s_n[a][2 * tid + 1] = pn1;
+        }
+        __syncthreads();
+        plan(a, 0);
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+    // ---- per-rotation totals
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         kept += __shfl_xor_sync(0xffffffffu, kept, d);
@@ -352,21 +486,19 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 16 ? 1 : ITEMS >= 8 ? 3 :
     if (lane == 0) { s_red[0][warp] = kept; s_red[1][warp] = cre; s_red[2][warp] = alive; }
     if (over) atomicOr(&S->err, ERR_OVERFLOW);
     __syncthreads();
-    int *OCNT = A.cnt[cur ^ 1];
-    BkRec &me = A.rec[r + 1];
-    if (tid < 2 * G) OCNT[s_b[tid]] = min(s_out[tid], CAP);
     if (tid == 0) {
-        int kt = 0, ct = 0, at = 0, mx = 0;
+        BkRec &me = A.rec[r + 1];
+        int kt = 0, ct = 0, at = 0;
         for (int w = 0; w < T / 32; ++w) { kt += s_red[0][w]; ct += s_red[1][w]; at += s_red[2][w]; }
-        for (int b = 0; b < 2 * G; ++b) mx = max(mx, s_out[b]);
         atomicAdd(&me.n_out, (unsigned long long)kt);
         atomicAdd(&me.created, (unsigned long long)ct);
         if (pref) atomicAdd(&me.np, (unsigned long long)at);
-        atomicMax(&me.maxcnt, mx);
-        if (mx > CAP) {
+        atomicMax(&me.maxcnt, s_mx);
+        if (s_mx > CAP) {
             atomicOr(&S->err, ERR_OVERFLOW);
             atomicMin(&S->bk_fail, r);
         }
+        if (s_bad) atomicOr(&S->err, ERR_BOUNDS);
     }
 }
 
@@ -392,6 +524,10 @@ __global__ void k_bk_scatter(const u64 *SZ, const u64 *SX, const double *SC, lon
         if (scnt && (int)(i % cap) >= scnt[i / cap]) continue;
         const Key<NW> kk = load_key<NW>(SZ, SX, i);
         const unsigned b = bk_hash<NW>(kk.z, kk.x, rows, dbits);
+        if (b >= (1u << dbits)) {
+            atomicOr(err, ERR_BOUNDS);
+            continue;
+        }
         const int pos = atomicAdd(&dcnt[b], 1);
         if (pos >= cap) {
             atomicOr(err, ERR_OVERFLOW);
@@ -422,13 +558,17 @@ __global__ void __launch_bounds__(BKS_THREADS) k_bk_offsets(const int *cnt, int 
 // Gather of a bucket layout into a dense array (one warp per bucket).
 template <int NW>
 __global__ void k_bk_gather(const u64 *SZ, const u64 *SX, const double *SC, const int *cnt, int nb, int cap,
-                            const long long *off, u64 *DZ, u64 *DX, double *DC) {
+                            const long long *off, u64 *DZ, u64 *DX, double *DC, long long dcap, DevState *S) {
     const int lane = threadIdx.x & 31;
     const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long b = w0; b < nb; b += nw) {
         const int m = min(cnt[b], cap);
         const long long o = off[b];
+        if (o < 0 || o + m > dcap) {
+            if (lane == 0) flag_bounds(S, 9, o);
+            continue;
+        }
         for (int j = lane; j < m; j += 32) {
             const long long s = b * cap + j;
             store_key<NW>(DZ, DX, o + j, load_key<NW>(SZ, SX, s));

@@ -26,10 +26,10 @@ from . import _lib
 from .circuits import lattice64
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tuning")
-VARIANTS = [(128, 4), (256, 4), (256, 8), (512, 8), (512, 16), (1024, 16)]
+VARIANTS = [(128, 4), (256, 4), (512, 4), (256, 8), (512, 8), (1024, 8)]
 LOAD_DIVS = (4, 5, 6)
 CHUNKS = (32, 64, 128)
-DEFAULT = (256, 8, 5, 64)
+DEFAULT = (256, 4, 5, 64)
 
 _cache = {}
 
@@ -123,7 +123,7 @@ def tune(nws=(1, 2), quick=False, reps=2, log=print):
         cands = []
         # variants at the default load divisor and chunk, then the best variant's
         # load divisor and chunk
-        for cap, items in (VARIANTS if not quick else [(256, 8), (512, 8)]):
+        for cap, items in (VARIANTS if not quick else [(256, 4), (512, 4)]):
             t = (cap, items, DEFAULT[2], DEFAULT[3])
             cands.append((t, _time_one(nw, t, reps)))
             log(f"nw={nw} {t}: {cands[-1][1]:.4g} terms/s")
