@@ -821,7 +821,7 @@ static constexpr int BK_MIN_ROT = 32;     // shorter sequences keep the sorted-m
 // give the same result; the switch exists for comparisons).
 static bool bk_enabled() {
     const char *e = getenv("PAULIPROP_WINDOW1_PATH");
-    return e && strcmp(e, "buckets") == 0;
+    return !(e && strcmp(e, "tiles") == 0);
 }
 
 // Compiled variants of k_bk_rotate: (bucket capacity, staged items per thread).
