@@ -84,14 +84,23 @@ __device__ __forceinline__ unsigned bk_hash(const u64 *kz, const u64 *kx, const 
     return h;
 }
 
-// Slot hash of the shared-memory key index (a mix of all key bits).
+// Slot hash of the shared-memory key index: a 32-bit multiply-xor mix of all
+// key words (the terms of a group share their bucket-hash parities, not these).
 template <int NW, int TAB>
 __device__ __forceinline__ unsigned bk_slot(const Key<NW> &k) {
-    u64 h = k.z[0] * 0x9E3779B97F4A7C15ull ^ (k.x[0] + 0x632BE59BD9B4E019ull) * 0xC2B2AE3D27D4EB4Full;
-    if constexpr (NW == 2) h ^= k.z[1] * 0xD6E8FEB86659FD93ull ^ (k.x[1] + 0x165667B19E3779F9ull) * 0x94D049BB133111EBull;
-    h ^= h >> 31;
-    h *= 0xBF58476D1CE4E5B9ull;
-    return (unsigned)(h >> 40) & (TAB - 1);
+    unsigned h = (unsigned)k.z[0] ^ ((unsigned)(k.z[0] >> 32) * 0x9E3779B1u);
+    h = h * 0x85EBCA77u ^ (unsigned)k.x[0];
+    h = h * 0xC2B2AE3Du ^ (unsigned)(k.x[0] >> 32);
+    if constexpr (NW == 2) {
+        h = h * 0x27D4EB2Fu ^ (unsigned)k.z[1];
+        h = h * 0x165667B1u ^ (unsigned)(k.z[1] >> 32);
+        h = h * 0x9E3779B1u ^ (unsigned)k.x[1];
+        h = h * 0x85EBCA77u ^ (unsigned)(k.x[1] >> 32);
+    }
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h & (TAB - 1);
 }
 
 // Shared memory of k_bk_rotate: two staging areas (keys, coefficients, local
@@ -161,7 +170,7 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
     constexpr int GMAX = bk_group_max<CAP, ITEMS>();
     constexpr int NBK = 2 * GMAX;                  // buckets of a group
     static_assert(2 * CAP <= SMI, "a pair of full buckets fits");
-    static_assert(NBK <= 256, "local bucket index fits a byte");
+    static_assert(NBK <= 32, "one warp handles a group's buckets");
     DevState *S = A.S;
     if (S->err) return;
     const long long r = S->bk_rot0 + k;
@@ -361,12 +370,11 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
                     const int j = find(qk);
                     if (j >= ntot) flag_bounds(S, 8, j);
                     if (j >= 0 && j < ntot && !sdead[j]) {
-                        // the partner's sin branch lands on this key: live value first, then the append
-                        const Key<NW> kj = skey(a, j);
-                        Key<NW> back;
-                        double sgj = 0.0;
-                        rotate_term<NW>(kj, g, &back, &sgj);
-                        const double t = __dmul_rn(sgj * sv, sc[a][j]);
+                        // the partner's sin branch lands on this key: live value first, then
+                        // the append.  Its phase factor is -sg: for Q = P xor G,
+                        // k(P) + k(Q) = 2 (m1(P) + m1(Q) - ng) = 4 (m1(P) - popc(gx & gz & zP))
+                        // (mod 4) in _rotate_range!'s k (spv_kernels.jl:162-163), and k is odd
+                        const double t = __dmul_rn(-(sg * sv), sc[a][j]);
                         if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
                     } else if (s_ok && !should_drop<NW>(P.strict, qk, fabs(s))) {
                         nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
@@ -451,28 +459,30 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
             cp_async_wait<0>();
             __syncthreads();
         }
-        // output counts of the group's buckets
-        if (tid < 2 * G) {
-            const int m = s_out[tid];
-            A.cnt[cur ^ 1][s_b[a][tid]] = min(m, CAP);
-            atomicMax(&s_mx, m);
-            s_out[tid] = 0;
-        }
-        __syncthreads();
-        // area a now takes the group after next
-        if (tid < G) {
-            if (gafter < ngroups) {
-                if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
-                    flag_bounds(S, 10, ((long long)pn0 << 20) | (pn1 & 0xfffff));
-                    s_bad = 1;
-                    pb0 = pb1 = pn0 = pn1 = 0;
-                }
+        // output counts of the group's buckets, then area a takes the group after
+        // next and is planned (warp 0 alone: 2 * G <= 32)
+        if (warp == 0) {
+            if (lane < 2 * G) {
+                const int m = s_out[lane];
+                A.cnt[cur ^ 1][s_b[a][lane]] = min(m, CAP);
+                atomicMax(&s_mx, m);
+                s_out[lane] = 0;
             }
-            s_b[a][2 * tid] = pb0; s_b[a][2 * tid + 1] = pb1;
-            s_n[a][2 * tid] = pn0; s_n[a][2 * tid + 1] = pn1;
+            __syncwarp();
+            if (lane < G) {
+                if (gafter < ngroups) {
+                    if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
+                        flag_bounds(S, 10, ((long long)pn0 << 20) | (pn1 & 0xfffff));
+                        s_bad = 1;
+                        pb0 = pb1 = pn0 = pn1 = 0;
+                    }
+                }
+                s_b[a][2 * lane] = pb0; s_b[a][2 * lane + 1] = pb1;
+                s_n[a][2 * lane] = pn0; s_n[a][2 * lane + 1] = pn1;
+            }
+            __syncwarp();
+            plan(a, 0);
         }
-        __syncthreads();
-        plan(a, 0);
         __syncthreads();
     }
     cp_async_wait<0>();
