@@ -42,6 +42,9 @@ constexpr int BK_ROWS = 26;                    // hash rows: at most 2^26 bucket
 constexpr int BK_THREADS = 256;
 constexpr int BK_DEFAULT_CAP = 256;
 constexpr int BK_DEFAULT_ITEMS = 4;
+#ifndef BK_MIN_BLOCKS
+#define BK_MIN_BLOCKS 3                        // resident CTAs per SM the register budget aims at (4-item variants)
+#endif
 
 // Per-rotation record: rec[r] describes the live set entering rotation r (the
 // output of rotation r - 1); rotation r reads it and fills rec[r + 1].
@@ -142,6 +145,43 @@ __device__ __forceinline__ int bk_claim(int *s_out, int lb, bool want) {
     return pos;
 }
 
+// The common criteria of a compiled filter in registers (coefficient
+// threshold, weight and X-weight caps); a filter that also uses the Majorana
+// weight, a damped threshold or the batched word mask is evaluated in full.
+struct FQuick {
+    double thresh;
+    int wmax, xwmax, full;
+};
+
+__device__ __forceinline__ FQuick fquick(const DevFilter &f) {
+    FQuick q;
+    q.thresh = f.thresh;
+    q.wmax = (int)min(f.wmax, 1ll << 30);
+    q.xwmax = (int)min(f.xwmax, 1ll << 30);
+    q.full = (f.use_mw || f.use_dw || f.use_dxw || f.wlow) ? 1 : 0;
+    return q;
+}
+
+// should_drop (spv_kernels.jl:64-79) through FQuick.
+template <int NW>
+__device__ __forceinline__ bool drop_q(const FQuick &q, const DevFilter &f, const Key<NW> &k, double absc) {
+    if (q.full) return should_drop<NW>(f, k, absc);
+    if (absc <= q.thresh) return true;
+    int wt = 0, xw = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) { wt += __popcll(k.z[w] | k.x[w]); xw += __popcll(k.x[w]); }
+    return wt > q.wmax || xw > q.xwmax;
+}
+
+// P anticommutes with G (the parity test of rotate_term).
+template <int NW>
+__device__ __forceinline__ bool anticommutes(const Key<NW> &p, const GenRec &g) {
+    int m = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) m += __popcll(g.gx[w] & p.z[w]) + __popcll(g.gz[w] & p.x[w]);
+    return (m & 1) != 0;
+}
+
 // Buckets of pair p: (b0, b0 xor delta), or (2p, 2p + 1) when delta = 0.
 __device__ __forceinline__ void bk_pair(unsigned delta, long long p, int *b0, int *b1) {
     if (delta == 0) {
@@ -163,7 +203,7 @@ __device__ __forceinline__ void bk_pair(unsigned delta, long long p, int *b0, in
 // rotation's index within the launched graph (rotation S->bk_rot0 + k, input set
 // (S->bk_cur0 + k) & 1).
 template <int NW, int CAP, int ITEMS>
-__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(BkArgs A, int k) {
+__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_bk_rotate(BkArgs A, int k) {
     constexpr int T = BK_THREADS;
     constexpr int SMI = T * ITEMS;                 // staged terms per area
     constexpr int TAB = 2 * SMI;                   // key index slots
@@ -237,6 +277,7 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
     const DevParams &P = *A.P;
     const bool do_chan = (g.flags & GEN_CHANNEL) != 0 && P.chan_kind >= 0;
     const bool local_on = P.local_active != 0;
+    const FQuick fs = fquick(P.strict);
     const double cv = g.cosv, sv = g.sinv;
     const int flip = delta != 0 ? 1 : 0;
 
@@ -285,25 +326,28 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
             if (tid == 0) flag_bounds(S, 5, ((long long)ntot << 16) | nloc);
             return;
         }
-        for (int i = tid; i < ntot; i += T) {
-            int lb = 0;
-            while (lb + 1 < nloc && s_off[a][lb + 1] <= i) ++lb;
+        // warp w copies buckets w, w + 8, ... (each a contiguous run of slots)
+        for (int lb = warp; lb < nloc; lb += T / 32) {
             const int bq = s_b[a][2 * j0 + lb];
-            const long long p = (long long)bq * CAP + (i - s_off[a][lb]);
-            if (bq < 0 || bq >= nb || i - s_off[a][lb] >= CAP) {
-                flag_bounds(S, 6, p);
-                sbk[i] = 0;
+            const int o0 = s_off[a][lb], cnt = s_off[a][lb + 1] - o0;
+            if (bq < 0 || bq >= nb || cnt < 0 || cnt > CAP) {
+                if (lane == 0) flag_bounds(S, 6, ((long long)bq << 20) | (cnt & 0xfffff));
+                for (int t = lane; t < cnt; t += 32) sbk[o0 + t] = 0;
                 continue;
             }
-            if constexpr (NW == 1) {
-                cp_async8(skz[a] + i, Z + p);
-                cp_async8(skx[a] + i, X + p);
-            } else {
-                cp_async16(skz[a] + 2 * i, Z + 2 * p);
-                cp_async16(skx[a] + 2 * i, X + 2 * p);
+            for (int t = lane; t < cnt; t += 32) {
+                const int i = o0 + t;
+                const long long p = (long long)bq * CAP + t;
+                if constexpr (NW == 1) {
+                    cp_async8(skz[a] + i, Z + p);
+                    cp_async8(skx[a] + i, X + p);
+                } else {
+                    cp_async16(skz[a] + 2 * i, Z + 2 * p);
+                    cp_async16(skx[a] + 2 * i, X + 2 * p);
+                }
+                cp_async8(sc[a] + i, C + p);
+                sbk[i] = (unsigned char)(2 * j0 + lb);
             }
-            cp_async8(sc[a] + i, C + p);
-            sbk[i] = (unsigned char)(2 * j0 + lb);
         }
     };
     int cre = 0, alive = 0, kept = 0;
@@ -321,15 +365,19 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
             __syncthreads();
             return;
         }
-        // index the keys; mark the terms the early merge drops
+        // mark the terms the early merge drops, and index the live terms that
+        // anticommute with G: only they can be a partner (P xor G anticommutes
+        // exactly when P does), and a dropped partner counts as absent
         for (int i = tid; i < ntot; i += T) {
             const Key<NW> kk = skey(a, i);
+            const bool dead = pref && drop_q<NW>(fs, P.strict, kk, fabs(sc[a][i]));
+            sdead[i] = dead ? 1 : 0;
+            if (dead || !anticommutes<NW>(kk, g)) continue;
             unsigned h = bk_slot<NW, TAB>(kk);
             for (int probe = 0; probe < TAB; ++probe) {
                 if (atomicCAS(&tab[h], 0u, (unsigned)(i + 1)) == 0u) break;
                 h = (h + 1) & (TAB - 1);
             }
-            sdead[i] = (pref && should_drop<NW>(P.strict, kk, fabs(sc[a][i]))) ? 1 : 0;
         }
         __syncthreads();
         auto find = [&](const Key<NW> &q) {
@@ -369,19 +417,19 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : 3) k_bk_rotate(Bk
                     cre += s_ok ? 1 : 0;
                     const int j = find(qk);
                     if (j >= ntot) flag_bounds(S, 8, j);
-                    if (j >= 0 && j < ntot && !sdead[j]) {
+                    if (j >= 0 && j < ntot) {
                         // the partner's sin branch lands on this key: live value first, then
                         // the append.  Its phase factor is -sg: for Q = P xor G,
                         // k(P) + k(Q) = 2 (m1(P) + m1(Q) - ng) = 4 (m1(P) - popc(gx & gz & zP))
                         // (mod 4) in _rotate_range!'s k (spv_kernels.jl:162-163), and k is odd
                         const double t = __dmul_rn(-(sg * sv), sc[a][j]);
                         if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
-                    } else if (s_ok && !should_drop<NW>(P.strict, qk, fabs(s))) {
+                    } else if (s_ok && !drop_q<NW>(fs, P.strict, qk, fabs(s))) {
                         nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
                         nw_ = true;
                     }
                 }
-                if (!should_drop<NW>(P.strict, kk, fabs(v))) {
+                if (!drop_q<NW>(fs, P.strict, kk, fabs(v))) {
                     oval = do_chan ? __dmul_rn(v, channel_factor<NW>(P, kk)) : v;
                     own = true;
                 }
