@@ -60,8 +60,10 @@ BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
 # dram__bytes_write.sum = 115.1 MB per launch against B(n + a + m) = 150.9 MB:
 # the gathered sin branches re-read live terms that are still in L2)
 MERGE_TRAFFIC_PER_ALG_BYTE = 115.09 / 150.88
-# DRAM traffic of k_bk_rotate per algorithmic byte: not captured yet
-BUCKET_TRAFFIC_PER_ALG_BYTE = None
+# DRAM traffic of k_bk_rotate<1,256,4> per algorithmic byte, from one ncu capture of
+# three launches of this workload at n = 1.90e6 live terms: (dram__bytes_read.sum +
+# dram__bytes_write.sum) = 86.9 MB per launch against B(n_in + n_out) = 91.0 MB
+BUCKET_TRAFFIC_PER_ALG_BYTE = 86.91 / 91.02
 
 
 def parse():
