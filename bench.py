@@ -723,10 +723,17 @@ def _measure(args, wname, ws, rank, local, dev, orc):
         dom_kernel = (f"k_bk_rotate<{nw},{tuning[0]},{tuning[1]}> (rotation + partner merge + filter + "
                       f"channel over bucket pairs)")
         traffic_ratio = BUCKET_TRAFFIC_PER_ALG_BYTE
-    else:
+    elif sp["t_merge"] > 0:
         dom_bytes, dom_launches = B * (sp["merge_in"] + sp["merge_out"]), len(gens)   # B*(n + a + m)
         dom_kernel = "k_merge<1,0> (merge + reduce-by-key + filter + channel + compaction)"
         traffic_ratio = MERGE_TRAFFIC_PER_ALG_BYTE if w.name == "lattice64" else None
+    else:
+        # the whole sequence ran in k_small_run (one CTA, the set in shared memory):
+        # its bytes are the step's B*(n + m), its time the step's
+        dom_bytes, dom_launches = pipe_bytes, 1
+        dom_kernel = f"k_small_run<{nw}> (whole sequence in one CTA)"
+        traffic_ratio = None
+        sp["t_merge"] = t / args.steps
     achieved = dom_bytes / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
     hbm, src = peaks()
 

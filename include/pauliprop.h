@@ -302,11 +302,12 @@ const char *pp_last_error(void);
  * reference; results do not depend on it).  (bucket_cap, items_per_thread) must be
  * a compiled variant: (128, 4), (256, 4), (512, 4), (256, 8), (512, 8) or
  * (1024, 8); a CTA of 256 threads has two staging areas of 256 * items_per_thread
- * terms (a group of bucket pairs in one, the next group's terms in the other).  load_div (3..16): bucketing aims at a mean load of at
- * most bucket_cap / load_div.  chunk (8..256): rotations launched between host
- * checks.  pauliprop's autotuner (pauliprop/tune.py) measures the variants on the
- * device and caches the fastest per (word count, SM count); a new handle starts
- * with (256, 4, 5, 64). */
+ * terms (a group of bucket pairs in one, the next group's terms in the other).
+ * load_div (3..16): bucketing aims at a mean load of at most bucket_cap /
+ * load_div.  chunk (8..256): rotations launched between host checks.
+ * pauliprop's autotuner (pauliprop/tune.py) measures the variants on the device
+ * and caches the fastest per (word count, SM count); a new handle starts with
+ * (512, 4, 6, 128). */
 typedef struct {
     int32_t bucket_cap, items_per_thread, load_div, chunk;
 } pp_tuning;
@@ -322,9 +323,14 @@ int pp_device_info(pp_spv *h, int32_t *sm_count, int32_t *cc_major, int32_t *cc_
  * transactional, so the handle keeps its previous live set.
  * pp_debug_lookback_timeout: runs one look-back wait on a status that nothing
  * publishes, bounded by limit polls (1..2^22); returns PP_TIMEOUT when the wait
- * gives up as it must, and the device stays usable. */
+ * gives up as it must, and the device stays usable.
+ * pp_debug_bucket_limit: bucket layouts of more than `slots` term slots count as
+ * not fitting in device memory (slots <= 0: only the real free memory limits
+ * them); a sequence whose live set outgrows the layout that fits continues on the
+ * sorted-merge kernels with the same result. */
 int pp_debug_fail_alloc(int64_t after);
 int pp_debug_lookback_timeout(int64_t limit);
+int pp_debug_bucket_limit(int64_t slots);
 
 #ifdef __cplusplus
 }

@@ -124,8 +124,8 @@ struct pp_spv {
     int *bk_aux = nullptr;                  // [0] largest scatter count, [1] scatter error bits
     std::unordered_map<int, cudaGraphExec_t> bk_graphs;   // key: bits * 4 + chunk class
     long long bk_graph_gen = -1;
-    pp_tuning tune = {BK_DEFAULT_CAP, BK_DEFAULT_ITEMS, 5, 64};   // pp_set_tuning
-    struct { int occ1 = 1, occ2 = 1; } bk_occ[8];                  // resident CTAs per SM of each variant
+    pp_tuning tune = {BK_DEFAULT_CAP, BK_DEFAULT_ITEMS, 6, 128};  // pp_set_tuning
+    struct { int occ1 = 1, occ2 = 1, occb = 1; } bk_occ[8];        // resident CTAs per SM of each variant
 };
 
 // ------------------------------------------------------------------ helpers
@@ -145,6 +145,9 @@ static void dfree(pp_spv *h, void *p) {
 // growth step succeeded, and the handle stays usable after an out-of-memory.
 // Test hook (pp_debug_fail_alloc): the k-th next device allocation fails.
 static std::atomic<long long> g_fail_alloc_after{0};
+// Test hook (pp_debug_bucket_limit): bucket layouts above this many term slots
+// count as not fitting in device memory (0: no limit).
+static std::atomic<long long> g_bk_slot_limit{0};
 
 template <typename T>
 static int dalloc(pp_spv *h, T **p, long long count) {
@@ -816,6 +819,10 @@ struct RunProf {
 // radix sort, so the live set is dense and sorted between calls as before.
 static int expect_dev(pp_spv *h, const u64 *k, double *out);
 static constexpr int BK_MIN_ROT = 32;     // shorter sequences keep the sorted-merge kernels
+// Internal status (never returned by the C ABI): a bucket layout for the live set
+// would not fit in device memory; the sequence continues on the sorted-merge
+// kernels from the rotation the device cursor is at.
+static constexpr int BK_NOFIT = 0x4b4e4f46;
 
 // PAULIPROP_WINDOW1_PATH=tiles selects the sorted-merge kernels instead (both
 // give the same result; the switch exists for comparisons).
@@ -827,13 +834,13 @@ static bool bk_enabled() {
 // Compiled variants of k_bk_rotate: (bucket capacity, staged items per thread).
 typedef void (*BkKernel)(BkArgs, int);
 struct BkVariant {
-    int cap, items, gmax;
-    BkKernel k1, k2;
+    int cap, items;
+    BkKernel k1, k2, kb;            // one- and two-word keys; batched instances (two-word)
     size_t smem1, smem2;
 };
 
 #define PP_BK_VARIANT(C, I)                                                                                 \
-    { C, I, bk_group_max<C, I>(), k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, bk_smem_bytes<1, C, I>(),     \
+    { C, I, k_bk_rotate<1, C, I>, k_bk_rotate<2, C, I>, k_bk_rotate<2, C, I, true>, bk_smem_bytes<1, C, I>(),     \
       bk_smem_bytes<2, C, I>() }
 static const BkVariant BK_VARIANTS[] = {PP_BK_VARIANT(128, 4), PP_BK_VARIANT(256, 4), PP_BK_VARIANT(512, 4),
                                         PP_BK_VARIANT(256, 8), PP_BK_VARIANT(512, 8), PP_BK_VARIANT(1024, 8)};
@@ -846,23 +853,15 @@ static const BkVariant *bk_variant(int cap, int items) {
     return nullptr;
 }
 
-// Bucket pairs per group for 2^bits buckets: about 0.6 of a staging area at the
-// typical load (a bucket averages about cap / 3.5 terms between splits), but
-// small enough that every resident CTA gets groups.
-static int bk_group_for(pp_spv *h, const BkVariant *v, int bits) {
-    const long long pairs = 1ll << (bits - 1);
-    const int want = std::max(1, (int)(1.05 * BK_THREADS * v->items / v->cap));
-    int gsz = 1;
-    while (gsz * 2 <= std::min(want, v->gmax) && pairs / (gsz * 2) >= 2ll * h->nsm) gsz *= 2;
-    return gsz;
-}
-
 template <int NW>
 static void bk_launch(pp_spv *h, const BkVariant *v, const BkArgs &A, int k) {
-    const long long groups = (1ll << (A.bits - 1)) / A.group;
-    const int occ = NW == 1 ? h->bk_occ[v - BK_VARIANTS].occ1 : h->bk_occ[v - BK_VARIANTS].occ2;
-    const int grid = (int)std::min(groups, (long long)h->nsm * occ);
-    (NW == 1 ? v->k1 : v->k2)<<<grid, BK_THREADS, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
+    // persistent grid: every resident CTA, or one per bucket pair (the kernel sizes its groups)
+    const long long pairs = 1ll << (A.bits - 1);
+    const auto &oc = h->bk_occ[v - BK_VARIANTS];
+    const bool batch = NW == 2 && h->batch_on;
+    const int occ = NW == 1 ? oc.occ1 : batch ? oc.occb : oc.occ2;
+    const int grid = (int)std::min(pairs, (long long)h->nsm * occ);
+    (NW == 1 ? v->k1 : batch ? v->kb : v->k2)<<<grid, BK_THREADS, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
 }
 
 // Hash rows: fixed pseudo-random words (splitmix64 from a fixed seed), so the
@@ -897,6 +896,10 @@ static int bk_rows_init(pp_spv *h) {
         h->bk_occ[i].occ1 = std::max(1, o);
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, v.k2, BK_THREADS, v.smem2));
         h->bk_occ[i].occ2 = std::max(1, o);
+        CU(cudaFuncSetAttribute(v.kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem2));
+        CU(cudaFuncSetAttribute(v.kb, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, v.kb, BK_THREADS, v.smem2));
+        h->bk_occ[i].occb = std::max(1, o);
     }
     return sync_check(h);
 }
@@ -915,12 +918,18 @@ static BkArgs bk_args(pp_spv *h, const BkVariant *v, int bits, BkRec *rec) {
     A.bits = bits;
     A.bits_cap = h->bk_bits_cap;
     A.rec_len = h->bk_rec_cap;
-    A.group = bk_group_for(h, v, bits);
     A.rows = h->bk_rows;
     A.rec = rec;
     A.S = h->S;
     A.P = h->P;
     A.gens = h->gens;
+    if (h->batch_on) {
+        A.bcos = h->bcos;
+        A.bsin = h->bsin;
+        A.bend = h->bend;
+        A.ninst = h->ninst;
+        A.ncol = h->ncol;
+    }
     return A;
 }
 
@@ -958,13 +967,16 @@ static int bk_reserve(pp_spv *h, int bits, int *cur, int cur_bits) {
     const int nbits = std::min(BK_ROWS, std::max(bits + 1, h->bk_cap == cap ? h->bk_bits_cap : 0));
     const long long slots = (long long)cap << nbits;
     {
+        // the two bucket sets, and room to convert a full layout (at most slots / 2
+        // terms before the next split) back to a dense sorted set, plus 4 GiB
         size_t freeb = 0, totalb = 0;
         if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) {
-            const double want = 2.0 * (double)slots * (16.0 * NW + 8.0);
-            if (want + 4.0 * (1ull << 30) > (double)freeb)
-                return fail(PP_OUT_OF_MEMORY, "bucketing " + std::to_string(slots) +
-                                                  " term slots would leave less than 4 GiB of device memory free");
+            const double B = 16.0 * NW + 8.0;
+            const double want = 2.0 * (double)slots * B + 1.5 * (double)slots * B;
+            if (want + 4.0 * (1ull << 30) > (double)freeb) return BK_NOFIT;
         }
+        const long long lim = g_bk_slot_limit.load();
+        if (lim > 0 && slots > lim) return BK_NOFIT;
     }
     u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
     double *nc[2] = {nullptr, nullptr};
@@ -1004,6 +1016,20 @@ static int bk_reserve(pp_spv *h, int bits, int *cur, int cur_bits) {
     h->bk_bits_cap = nbits;
     h->bk_cap = cap;
     return PP_OK;
+}
+
+// Frees the bucket sets (the live set is dense again).
+static void bk_release(pp_spv *h) {
+    for (int q = 0; q < 2; ++q) {
+        dfree(h, h->bkz[q]); dfree(h, h->bkx[q]); dfree(h, h->bkc[q]); dfree(h, h->bkcnt[q]);
+        h->bkz[q] = h->bkx[q] = nullptr;
+        h->bkc[q] = nullptr;
+        h->bkcnt[q] = nullptr;
+    }
+    dfree(h, h->bk_off);
+    h->bk_off = nullptr;
+    h->bk_bits_cap = -1;
+    h->buf_gen++;
 }
 
 // Moves the live bucket set *cur (2^*bits buckets) to a layout with more
@@ -1079,8 +1105,11 @@ static int bk_to_dense(pp_spv *h, int cur, int bits) {
 }
 
 // The window-1 sequence [start, L) on buckets.  The device cursor is at start.
+// per_rot: per-rotation times were asked for (each launch bracketed by events,
+// no graphs); otherwise the rotations replay from captured graphs, and a
+// profiled call (prof->on) times each graph replay.
 template <int NW>
-static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof, bool timed) {
+static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof, bool per_rot) {
     TRY(ensure_dense(h));
     TRY(bk_rows_init(h));
     const BkVariant *var = bk_variant(h->tune.bucket_cap, h->tune.items_per_thread);
@@ -1105,23 +1134,73 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
     // bucket the live set
     int bits = bk_bits_for(n0, h->tune.bucket_cap, h->tune.load_div), cur = 0;
     for (;;) {
-        TRY(bk_reserve<NW>(h, bits, &cur, -1));
+        const int rr = bk_reserve<NW>(h, bits, &cur, -1);
+        if (rr) return rr;                  // BK_NOFIT: nothing changed, the dense set is the input
         int mx = 0;
         TRY(bk_scatter<NW>(h, h->z[st.cur], h->x[st.cur], h->c[st.cur], n0, -1, 0, 0, bits, &mx));
         if (mx >= 0 && mx <= h->bk_cap / 2) break;
         if (++bits > BK_ROWS) return fail(PP_OUT_OF_MEMORY, "bucketed live set exceeds 2^26 buckets");
     }
+    cudaStream_t s = h->stream;
+    // totals and counters of rotations [start, upto) into the device state, and the
+    // live set (bucket set cur) back to the dense sorted layout
+    auto finish = [&](long long upto) -> int {
+        std::vector<BkRec> rec((size_t)(upto - start + 1));
+        CU(cudaMemcpyAsync(rec.data(), h->bk_rec + start, rec.size() * sizeof(BkRec), cudaMemcpyDeviceToHost, s));
+        TRY(sync_check(h));
+        TRY(read_state(h, &st));
+        std::vector<long long> rr;
+        if (h->rec_on) rr.assign((size_t)(4 * (upto - start)), 0);
+        for (long long r = start; r < upto; ++r) {
+            const BkRec &o = rec[(size_t)(r - start + 1)];
+            const long long n = o.n_in, a = (long long)o.created, tot = (long long)o.n_out, np = (long long)o.np;
+            st.live_in += n;
+            st.created += a;
+            st.merge_in += n + a;
+            st.merge_out += tot;
+            if (tot > st.peak) st.peak = tot;
+            if (o.pref) st.early += 1;
+            prof->bk_rot += 1;
+            prof->bk_bytes += (double)(16 * NW + 8) * (double)(n + tot);
+            if (h->rec_on) {
+                // WindowCounters of the rotation (window = 1): an early boundary merges
+                // n -> np first, the regular one np + a -> total
+                long long *q = &rr[(size_t)(4 * (r - start))];
+                q[0] = a;
+                q[1] = (o.pref ? n + np : n) + a;
+                q[2] = (o.pref ? np : 0) + tot;
+                q[3] = o.pref ? 1 : 0;
+            }
+        }
+        if (h->rec_on && upto > start)
+            CU(cudaMemcpy(h->rec + 4 * start, rr.data(), rr.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        {
+            // the early-merge capacity rule after the last rotation (as k_bk_rotate applies it)
+            const BkRec &o = rec.back();
+            long long acap = o.acap;
+            if (o.pref && (long long)o.np > acap) acap = std::max(2 * acap, (long long)o.np);
+            st.acap_logical = acap;
+        }
+        st.rot = upto;
+        TRY(write_state(h, &st));
+        return bk_to_dense<NW>(h, cur, bits);
+    };
     cur = 0;
     long long done = start;
-    cudaStream_t s = h->stream;
     const int chunk = h->tune.chunk;
+    std::vector<cudaEvent_t> gev;      // event pairs around the graph replays of a chunk (profiled calls)
+    struct GevGuard {
+        std::vector<cudaEvent_t> &v;
+        ~GevGuard() { for (auto e : v) cudaEventDestroy(e); }
+    } gevg{gev};
     while (done < L) {
         const long long len = std::min((long long)chunk, L - done);
         if (bits < 1 || bits > h->bk_bits_cap || h->bk_cap != var->cap || L + 1 > h->bk_rec_cap || (cur & ~1))
             return fail(PP_ERROR_EXCEPTION, "internal error: inconsistent bucket layout before a launch");
         k_bk_begin<<<1, 1, 0, s>>>(h->S, done, cur, 1);
         prof->launches += 1;
-        if (!timed) {
+        int ngraph = 0;
+        if (!per_rot) {
             long long r = 0;
             while (r < len) {
                 const int cls = (len - r >= chunk) ? 0 : (len - r >= 8) ? 1 : 2;
@@ -1133,7 +1212,16 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
                 }
                 cudaGraphExec_t ex = nullptr;
                 TRY(bk_graph<NW>(h, var, bits, cls, cl, &ex));
+                if (prof->on) {
+                    while ((int)gev.size() < 2 * (ngraph + 1)) {
+                        cudaEvent_t e;
+                        CU(cudaEventCreate(&e));
+                        gev.push_back(e);
+                    }
+                    CU(cudaEventRecord(gev[2 * ngraph], s));
+                }
                 CU(cudaGraphLaunch(ex, s));
+                if (prof->on) CU(cudaEventRecord(gev[2 * ngraph++ + 1], s));
                 prof->launches += cl;
                 r += cl;
             }
@@ -1158,6 +1246,11 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
             }
         }
         TRY(sync_check(h));
+        for (int q = 0; q < ngraph; ++q) {
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, gev[2 * q], gev[2 * q + 1]));
+            prof->t_merge += ms * 1e-3;
+        }
         TRY(read_state(h, &st));
         if (st.err & ~ERR_OVERFLOW) return check_err(h, st);   // the dense live set is the sequence's input
         const long long completed = (st.err & ERR_OVERFLOW) ? std::max(0ll, std::min(len, st.bk_fail - done)) : len;
@@ -1172,48 +1265,21 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
             TRY(write_state(h, &st));
             CU(cudaMemsetAsync(h->bk_rec + done + 1, 0, sizeof(BkRec), s));
         }
-        if (done < L && (over || last.maxcnt > h->bk_cap / 2)) TRY(bk_regrid<NW>(h, &cur, &bits));
-    }
-    // totals and counters of rotations [start, L)
-    std::vector<BkRec> rec((size_t)(L - start + 1));
-    CU(cudaMemcpyAsync(rec.data(), h->bk_rec + start, rec.size() * sizeof(BkRec), cudaMemcpyDeviceToHost, s));
-    TRY(sync_check(h));
-    TRY(read_state(h, &st));
-    std::vector<long long> rr;
-    if (h->rec_on) rr.assign((size_t)(4 * (L - start)), 0);
-    for (long long r = start; r < L; ++r) {
-        const BkRec &o = rec[(size_t)(r - start + 1)];
-        const long long n = o.n_in, a = (long long)o.created, tot = (long long)o.n_out, np = (long long)o.np;
-        st.live_in += n;
-        st.created += a;
-        st.merge_in += n + a;
-        st.merge_out += tot;
-        if (tot > st.peak) st.peak = tot;
-        if (o.pref) st.early += 1;
-        prof->bk_rot += 1;
-        prof->bk_bytes += (double)(16 * NW + 8) * (double)(n + tot);
-        if (h->rec_on) {
-            // WindowCounters of the rotation (window = 1): an early boundary merges
-            // n -> np first, the regular one np + a -> total
-            long long *q = &rr[(size_t)(4 * (r - start))];
-            q[0] = a;
-            q[1] = (o.pref ? n + np : n) + a;
-            q[2] = (o.pref ? np : 0) + tot;
-            q[3] = o.pref ? 1 : 0;
+        if (done < L && (over || last.maxcnt > h->bk_cap / 2)) {
+            const int rr = bk_regrid<NW>(h, &cur, &bits);
+            if (rr == BK_NOFIT) {
+                // no room for a larger layout: the rotations so far go back to the
+                // dense sorted set, the bucket sets are freed, and the sorted-merge
+                // kernels take the rest of the sequence
+                TRY(finish(done));
+                bk_release(h);
+                return BK_NOFIT;
+            }
+            if (rr) return rr;
         }
     }
-    if (h->rec_on && L > start)
-        CU(cudaMemcpy(h->rec + 4 * start, rr.data(), rr.size() * sizeof(long long), cudaMemcpyHostToDevice));
-    {
-        // the early-merge capacity rule after the last rotation (as k_bk_rotate applies it)
-        const BkRec &o = rec.back();
-        long long acap = o.acap;
-        if (o.pref && (long long)o.np > acap) acap = std::max(2 * acap, (long long)o.np);
-        st.acap_logical = acap;
-    }
-    st.rot = L;
-    TRY(write_state(h, &st));
-    TRY(bk_to_dense<NW>(h, cur, bits));
+    TRY(finish(L));
+    if (h->batch_on) return PP_OK;      // batched instances are measured per instance at their ends
     // <ket|O|ket> after the last rotation (GEN_MEASURE), on the sorted live set
     double ev = 0.0;
     TRY(expect_dev(h, h->Ph->ket, &ev));
@@ -1233,11 +1299,12 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
 template <int NW>
 static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof) {
     long long done = start;
-    const bool timed = prof->on || (ctr && (ctr->t_rotate || ctr->t_merge));
+    const bool per_rot = ctr && (ctr->t_rotate || ctr->t_merge);   // per-rotation times asked for
+    const bool timed = prof->on || per_rot;
     std::vector<cudaEvent_t> ev;   // 5 per rotation when timed
     bool table = false;            // the device segment table describes the (dense) live set
-    const bool small_ok = !timed && !h->batch_on && !h->Ph->local_active && h->Ph->corr_kind == 0;
-    const bool use_bk = bk_enabled() && !h->batch_on && h->Ph->corr_kind == 0;
+    const bool small_ok = !per_rot && !h->batch_on && !h->Ph->local_active && h->Ph->corr_kind == 0;
+    bool use_bk = bk_enabled() && h->Ph->corr_kind == 0;
     long long ncur = small_cap<NW>() + 1;   // live terms at the chunk's start (read when small_ok)
     if (small_ok) {
         DevState st;
@@ -1259,7 +1326,19 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
             done = st.rot;
             continue;
         }
-        if (use_bk && L - done >= BK_MIN_ROT) return run_bucket<NW>(h, done, L, ctr, prof, timed);
+        if (use_bk && L - done >= BK_MIN_ROT) {
+            const int rb = run_bucket<NW>(h, done, L, ctr, prof, per_rot);
+            if (rb != BK_NOFIT) return rb;
+            // no room for buckets: the rest of the sequence on the sorted-merge kernels,
+            // from the rotation the bucketed part reached
+            use_bk = false;
+            table = false;
+            DevState st;
+            TRY(read_state(h, &st));
+            done = st.rot;
+            ncur = small_ok ? st.n : small_cap<NW>() + 1;
+            continue;
+        }
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
@@ -1990,6 +2069,11 @@ extern "C" int pp_device_info(pp_spv *h, int32_t *sm_count, int32_t *cc_major, i
 // ------------------------------------------------------------------ test hooks
 extern "C" int pp_debug_fail_alloc(int64_t after) {
     g_fail_alloc_after.store(after > 0 ? after : 0);
+    return PP_OK;
+}
+
+extern "C" int pp_debug_bucket_limit(int64_t slots) {
+    g_bk_slot_limit.store(slots > 0 ? slots : 0);
     return PP_OK;
 }
 

@@ -40,11 +40,12 @@ namespace pp {
 // the other receives the next group's terms in the meantime.
 constexpr int BK_ROWS = 26;                    // hash rows: at most 2^26 buckets
 constexpr int BK_THREADS = 256;
-constexpr int BK_DEFAULT_CAP = 256;
+constexpr int BK_DEFAULT_CAP = 512;
 constexpr int BK_DEFAULT_ITEMS = 4;
-#ifndef BK_MIN_BLOCKS
-#define BK_MIN_BLOCKS 3                        // resident CTAs per SM the register budget aims at (4-item variants)
-#endif
+// Resident CTAs per SM the register budget aims at: four for one-word keys
+// (64 registers), three for two-word keys (at 64 they spill and run 10 % slower);
+// one for the 8-item variants, whose shared memory allows two at most.
+__host__ __device__ constexpr int bk_min_blocks(int nw, int items) { return items >= 8 ? 1 : nw == 1 ? 4 : 3; }
 
 // Per-rotation record: rec[r] describes the live set entering rotation r (the
 // output of rotation r - 1); rotation r reads it and fills rec[r + 1].
@@ -65,12 +66,17 @@ struct BkArgs {
     int bits;                       // 2^bits buckets
     int bits_cap;                   // the bucket sets and counts are allocated for 2^bits_cap buckets
     long long rec_len;              // entries of rec
-    int group;                      // bucket pairs per CTA (a power of two)
     const u64 *rows;                // [BK_ROWS][4]: z words 0..1, x words 0..1 of each hash row
     BkRec *rec;
     DevState *S;
     const DevParams *P;
     const GenRec *gens;
+    // batched instances (the instance index is z word 1 of every key): angle
+    // tables [instance][column] and the rotation each instance ends at
+    const double *bcos, *bsin;
+    const long long *bend;
+    long long ninst;
+    int ncol;
 };
 
 // Bucket of a key: the low `bits` bits of the GF(2)-linear hash.
@@ -107,14 +113,18 @@ __device__ __forceinline__ unsigned bk_slot(const Key<NW> &k) {
 }
 
 // Shared memory of k_bk_rotate: two staging areas (keys, coefficients, local
-// bucket of each term), the key index and the pre-filter flags.
+// bucket of each term) and the key index (16-bit slots, twice the area's terms).
 template <int NW, int CAP, int ITEMS>
 __host__ __device__ constexpr size_t bk_smem_bytes() {
-    return (size_t)(BK_THREADS * ITEMS) * (2 * (2 * NW * 8 + 8 + 1) + 2 * 4 + 1);
+    return (size_t)(BK_THREADS * ITEMS) * (2 * (2 * NW * 8 + 8 + 1) + 2 * 2);
 }
-// Bucket pairs a group may hold: the host picks a power of two up to this.
+// Most bucket pairs a group may hold (at most 16, so that one warp handles a
+// group's 32 buckets); the kernel picks the group size of each launch from the
+// mean bucket load.
 template <int CAP, int ITEMS>
-__host__ __device__ constexpr int bk_group_max() { return 2 * BK_THREADS * ITEMS / CAP; }
+__host__ __device__ constexpr int bk_group_max() {
+    return 4 * BK_THREADS * ITEMS / CAP < 16 ? 4 * BK_THREADS * ITEMS / CAP : 16;
+}
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -128,21 +138,27 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Position in output bucket lb for every lane that passes `want`: lanes of a warp
-// with the same bucket take consecutive slots from one shared-memory atomic.
-__device__ __forceinline__ int bk_claim(int *s_out, int lb, bool want) {
-    const unsigned act = __ballot_sync(0xffffffffu, want);
-    int pos = -1;
-    if (want) {
-        const unsigned peers = __match_any_sync(act, lb);
-        const int leader = __ffs(peers) - 1;
-        const int lane = threadIdx.x & 31;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&s_out[lb], __popc(peers));
-        base = __shfl_sync(peers, base, leader);
-        pos = base + __popc(peers & ((1u << lane) - 1u));
-    }
-    return pos;
+// Lanes of the warp whose local bucket equals this lane's: the staged terms of a
+// group lie in bucket order, so equal buckets form one run of consecutive lanes.
+__device__ __forceinline__ unsigned bk_segment(int lb, int lane) {
+    const int up = __shfl_up_sync(0xffffffffu, lb, 1);
+    const unsigned head = __ballot_sync(0xffffffffu, lane == 0 || up != lb);
+    const unsigned upto = 0xffffffffu >> (31 - lane);              // lanes 0 .. lane
+    const unsigned above = head & ~upto;
+    const int s0 = 31 - __clz(head & upto);
+    return (above ? (1u << (__ffs(above) - 1)) - 1u : 0xffffffffu) & ~((1u << s0) - 1u);
+}
+
+// Position in output bucket ob for every lane that passes `want` (ob is the same
+// across a segment): the segment's first wanting lane takes consecutive slots
+// for all of them from one shared-memory atomic.
+__device__ __forceinline__ int bk_claim(int *s_out, int ob, bool want, unsigned seg, int lane) {
+    const unsigned peers = __ballot_sync(0xffffffffu, want) & seg;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (want && lane == leader) base = atomicAdd(&s_out[ob], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader < 0 ? lane : leader);
+    return want ? base + __popc(peers & ((1u << lane) - 1u)) : -1;
 }
 
 // The common criteria of a compiled filter in registers (coefficient
@@ -195,15 +211,24 @@ __device__ __forceinline__ void bk_pair(unsigned delta, long long p, int *b0, in
 }
 
 // One window-1 rotation.  The grid is persistent: CTA c processes the groups
-// c, c + gridDim.x, ... of `group` consecutive bucket pairs, and while it
-// processes one group its copies of the next group's terms are in flight
-// (cp.async into the other staging area).  A group whose terms exceed the
-// staging area is processed in sub-groups of consecutive pairs, loaded in turn
-// (a single pair always fits: 2 * CAP <= BK_THREADS * ITEMS).  k is the
+// c, c + gridDim.x, ... of G consecutive bucket pairs, and while it processes one
+// group its copies of the next group's terms are in flight (cp.async into the
+// other staging area).  G is the largest power of two up to GMAX whose expected
+// terms stay within 3/4 of a staging area at the entering set's mean bucket load
+// and that leaves every CTA a group.  A group whose terms exceed the staging
+// area is processed in sub-groups of consecutive pairs, loaded in turn (a single
+// pair always fits: 2 * CAP <= BK_THREADS * ITEMS).  Three block barriers per
+// group: staged terms visible, key index built, outputs claimed.  k is the
 // rotation's index within the launched graph (rotation S->bk_rot0 + k, input set
 // (S->bk_cur0 + k) & 1).
-template <int NW, int CAP, int ITEMS>
-__global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_bk_rotate(BkArgs A, int k) {
+//
+// BATCH (two-word keys only): the live set holds many instances, instance i's
+// terms carrying i in z word 1, which no generator changes, so a term's partner
+// is in its own instance.  Each term rotates by its instance's angle column; a
+// term whose instance has ended is kept as it is (no rotation, no filter, no
+// channel) until it is harvested.
+template <int NW, int CAP, int ITEMS, bool BATCH = false>
+__global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rotate(BkArgs A, int k) {
     constexpr int T = BK_THREADS;
     constexpr int SMI = T * ITEMS;                 // staged terms per area
     constexpr int TAB = 2 * SMI;                   // key index slots
@@ -211,8 +236,14 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
     constexpr int NBK = 2 * GMAX;                  // buckets of a group
     static_assert(2 * CAP <= SMI, "a pair of full buckets fits");
     static_assert(NBK <= 32, "one warp handles a group's buckets");
+    static_assert(SMI < 0x10000, "16-bit key index entries");
+    static_assert(!BATCH || NW == 2, "batched instances use two-word keys");
     DevState *S = A.S;
-    if (S->err) return;
+    // one read of the error word for the whole CTA (another CTA may set it meanwhile)
+    __shared__ int s_err;
+    if (threadIdx.x == 0) s_err = S->err;
+    __syncthreads();
+    if (s_err) return;
     const long long r = S->bk_rot0 + k;
     if (r >= S->rot_end) return;
     const int cur = (S->bk_cur0 + k) & 1;
@@ -222,18 +253,15 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
     __shared__ int s_out[NBK], s_mx, s_bad;
     __shared__ int s_red[3][T / 32];
     extern __shared__ u64 bsm[];
-    // staging area a: keys (NW words each, z then x), coefficients, local buckets
-    u64 *skz[2], *skx[2];
-    double *sc[2];
-    skz[0] = bsm;
-    skx[0] = skz[0] + NW * SMI;
-    sc[0] = reinterpret_cast<double *>(skx[0] + NW * SMI);
-    skz[1] = reinterpret_cast<u64 *>(sc[0] + SMI);
-    skx[1] = skz[1] + NW * SMI;
-    sc[1] = reinterpret_cast<double *>(skx[1] + NW * SMI);
-    unsigned *tab = reinterpret_cast<unsigned *>(sc[1] + SMI);           // [TAB]
-    unsigned char *sbk0 = reinterpret_cast<unsigned char *>(tab + TAB);  // [2][SMI]
-    unsigned char *sdead = sbk0 + 2 * SMI;                               // [SMI]
+    // staging area a: keys (NW words each, z then x), coefficients; then the key
+    // index and, per area, each staged term's local bucket (bit 7: dropped by the
+    // early merge)
+    constexpr int AREA = (2 * NW + 1) * SMI;       // u64 words of one staging area
+    auto skz = [&](int a) { return bsm + a * AREA; };
+    auto skx = [&](int a) { return bsm + a * AREA + NW * SMI; };
+    auto sc = [&](int a) { return reinterpret_cast<double *>(bsm + a * AREA + 2 * NW * SMI); };
+    unsigned short *tab = reinterpret_cast<unsigned short *>(bsm + 2 * AREA);   // [TAB]
+    unsigned char *sbk0 = reinterpret_cast<unsigned char *>(tab + TAB);        // [2][SMI]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         g = A.gens[r];
@@ -258,22 +286,29 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
         me.acap = acap;
         me.pref = pref ? 1 : 0;
     }
-    for (int i = tid; i < TAB; i += T) tab[i] = 0u;
+    {
+        uint4 *t4 = reinterpret_cast<uint4 *>(tab);
+        for (int i = tid; i < TAB / 8; i += T) t4[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     if (tid < NBK) s_out[tid] = 0;
     __syncthreads();
     const unsigned delta = s_delta;
     const long long nb = 1ll << A.bits;
-    const int G = A.group;
-    const long long ngroups = (nb / 2) / G;
-    if (G < 1 || G > GMAX || (nb / 2) % G != 0 || A.bits > A.bits_cap || A.bits < 1) {
+    const long long pairs = nb / 2;
+    int G = GMAX;
+    while (G > 1 && (8ll * G * n_r > 3ll * SMI * nb || pairs / G < (long long)gridDim.x)) G >>= 1;
+    const long long ngroups = pairs / G;
+    if (A.bits > A.bits_cap || A.bits < 1 || pairs % G != 0) {
         if (tid == 0) flag_bounds(S, 1, ((long long)A.bits << 16) | G);
         return;
     }
-    const int *CNT = A.cnt[cur];
-    const u64 *Z = A.z[cur], *X = A.x[cur];
-    const double *C = A.c[cur];
-    u64 *OZ = A.z[cur ^ 1], *OX = A.x[cur ^ 1];
-    double *OC = A.c[cur ^ 1];
+    // (selected, not indexed: a runtime index into the parameter struct would copy it to the stack)
+    const int *CNT = cur ? A.cnt[1] : A.cnt[0];
+    int *OCNT = cur ? A.cnt[0] : A.cnt[1];
+    const u64 *Z = cur ? A.z[1] : A.z[0], *X = cur ? A.x[1] : A.x[0];
+    const double *C = cur ? A.c[1] : A.c[0];
+    u64 *OZ = cur ? A.z[0] : A.z[1], *OX = cur ? A.x[0] : A.x[1];
+    double *OC = cur ? A.c[0] : A.c[1];
     const DevParams &P = *A.P;
     const bool do_chan = (g.flags & GEN_CHANNEL) != 0 && P.chan_kind >= 0;
     const bool local_on = P.local_active != 0;
@@ -332,21 +367,21 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
             const int o0 = s_off[a][lb], cnt = s_off[a][lb + 1] - o0;
             if (bq < 0 || bq >= nb || cnt < 0 || cnt > CAP) {
                 if (lane == 0) flag_bounds(S, 6, ((long long)bq << 20) | (cnt & 0xfffff));
-                for (int t = lane; t < cnt; t += 32) sbk[o0 + t] = 0;
+                for (int t = lane; t < cnt; t += 32) sbk[o0 + t] = (unsigned char)lb;
                 continue;
             }
             for (int t = lane; t < cnt; t += 32) {
                 const int i = o0 + t;
                 const long long p = (long long)bq * CAP + t;
                 if constexpr (NW == 1) {
-                    cp_async8(skz[a] + i, Z + p);
-                    cp_async8(skx[a] + i, X + p);
+                    cp_async8(skz(a) + i, Z + p);
+                    cp_async8(skx(a) + i, X + p);
                 } else {
-                    cp_async16(skz[a] + 2 * i, Z + 2 * p);
-                    cp_async16(skx[a] + 2 * i, X + 2 * p);
+                    cp_async16(skz(a) + 2 * i, Z + 2 * p);
+                    cp_async16(skx(a) + 2 * i, X + 2 * p);
                 }
-                cp_async8(sc[a] + i, C + p);
-                sbk[i] = (unsigned char)(2 * j0 + lb);
+                cp_async8(sc(a) + i, C + p);
+                sbk[i] = (unsigned char)lb;
             }
         }
     };
@@ -355,27 +390,33 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
     auto skey = [&](int a, int i) {
         Key<NW> kk;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) { kk.z[w] = skz[a][NW * i + w]; kk.x[w] = skx[a][NW * i + w]; }
+        for (int w = 0; w < NW; ++w) { kk.z[w] = skz(a)[NW * i + w]; kk.x[w] = skx(a)[NW * i + w]; }
         return kk;
     };
-    // process the staged sub-group of area a (ntot terms); leaves the index clear
-    auto run = [&](int a, int ntot) {
-        const unsigned char *sbk = sbk0 + a * SMI;
+    // process the staged sub-group [j0, j1) of area a; leaves the index clear and
+    // returns j1.  The plan of area a is read here, before the first barrier: once
+    // the outputs are claimed (the last barrier) the area may be planned anew.
+    auto run = [&](int a, int j0) {
+        unsigned char *sbk = sbk0 + a * SMI;
+        const int j1 = s_j1[a];
+        const int ntot = s_off[a][2 * (j1 - j0)];
         if (ntot > SMI) {                    // uniform: skipped by every thread (flagged in issue)
             __syncthreads();
-            return;
+            return j1;
         }
         // mark the terms the early merge drops, and index the live terms that
         // anticommute with G: only they can be a partner (P xor G anticommutes
         // exactly when P does), and a dropped partner counts as absent
         for (int i = tid; i < ntot; i += T) {
             const Key<NW> kk = skey(a, i);
-            const bool dead = pref && drop_q<NW>(fs, P.strict, kk, fabs(sc[a][i]));
-            sdead[i] = dead ? 1 : 0;
-            if (dead || !anticommutes<NW>(kk, g)) continue;
+            if (pref && drop_q<NW>(fs, P.strict, kk, fabs(sc(a)[i]))) {
+                sbk[i] |= 0x80;
+                continue;
+            }
+            if (!anticommutes<NW>(kk, g)) continue;
             unsigned h = bk_slot<NW, TAB>(kk);
             for (int probe = 0; probe < TAB; ++probe) {
-                if (atomicCAS(&tab[h], 0u, (unsigned)(i + 1)) == 0u) break;
+                if (atomicCAS(&tab[h], (unsigned short)0, (unsigned short)(i + 1)) == (unsigned short)0) break;
                 h = (h + 1) & (TAB - 1);
             }
         }
@@ -383,10 +424,9 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
         auto find = [&](const Key<NW> &q) {
             unsigned h = bk_slot<NW, TAB>(q);
             for (int probe = 0; probe < TAB; ++probe) {
-                const unsigned e = tab[h];
-                if (e == 0u) return -1;
-                const int j = (int)e - 1;
-                if (key_eq<NW>(skey(a, j), q)) return j;
+                const int e = tab[h];
+                if (e == 0) return -1;
+                if (key_eq<NW>(skey(a, e - 1), q)) return e - 1;
                 h = (h + 1) & (TAB - 1);
             }
             return -1;
@@ -394,25 +434,42 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
         const int rounds = (ntot + T - 1) / T;
         for (int rd = 0; rd < rounds; ++rd) {
             const int i = rd * T + tid;
-            const bool in = i < ntot && !sdead[i];
+            // local bucket (0x7f past the staged terms keeps buckets nondecreasing
+            // across the warp) and early-merge drop flag
+            const int tag = i < ntot ? sbk[i] : 0x7f;
+            int lb = tag & 0x7f;
+            const bool in = i < ntot && tag < 0x80;
+            if (i < ntot && lb >= 2 * (j1 - j0)) {
+                flag_bounds(S, 7, lb);
+                lb = 0;
+            }
             bool own = false, nw_ = false;
             double oval = 0.0, nval = 0.0;
-            int lb = 0;
             if (in) {
                 ++alive;
-                lb = sbk[i];
-                if (lb >= 2 * G) {
-                    flag_bounds(S, 7, lb);
-                    lb = 0;
-                }
                 const Key<NW> kk = skey(a, i);
-                const double c = sc[a][i];
+                const double c = sc(a)[i];
                 double v = c;
                 Key<NW> qk;
                 double sg = 0.0;
-                if (rotate_term<NW>(kk, g, &qk, &sg)) {
-                    v = __dmul_rn(c, cv);
-                    const double s = __dmul_rn(sg * sv, c);      // (k - 2) * sin(theta) * c, spv_kernels.jl:163
+                double cvt = cv, svt = sv;
+                bool act = true;                                 // the term's instance is running
+                if constexpr (BATCH) {
+                    const u64 t = kk.z[NW - 1];
+                    if (t >= (u64)A.ninst) {
+                        flag_bounds(S, 11, (long long)t);
+                        act = false;
+                    } else if (r >= A.bend[t]) {
+                        act = false;
+                    } else {
+                        const long long ai = (long long)t * A.ncol + g.acol;
+                        cvt = A.bcos[ai];
+                        svt = A.bsin[ai];
+                    }
+                }
+                if (act && rotate_term<NW>(kk, g, &qk, &sg)) {
+                    v = __dmul_rn(c, cvt);
+                    const double s = __dmul_rn(sg * svt, c);     // (k - 2) * sin(theta) * c, spv_kernels.jl:163
                     const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
                     cre += s_ok ? 1 : 0;
                     const int j = find(qk);
@@ -422,31 +479,36 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
                         // the append.  Its phase factor is -sg: for Q = P xor G,
                         // k(P) + k(Q) = 2 (m1(P) + m1(Q) - ng) = 4 (m1(P) - popc(gx & gz & zP))
                         // (mod 4) in _rotate_range!'s k (spv_kernels.jl:162-163), and k is odd
-                        const double t = __dmul_rn(-(sg * sv), sc[a][j]);
+                        const double t = __dmul_rn(-(sg * svt), sc(a)[j]);
                         if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
                     } else if (s_ok && !drop_q<NW>(fs, P.strict, qk, fabs(s))) {
                         nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
                         nw_ = true;
                     }
                 }
-                if (!drop_q<NW>(fs, P.strict, kk, fabs(v))) {
+                if (!act) {
+                    oval = v;                                    // an ended instance is kept as it is
+                    own = true;
+                } else if (!drop_q<NW>(fs, P.strict, kk, fabs(v))) {
                     oval = do_chan ? __dmul_rn(v, channel_factor<NW>(P, kk)) : v;
                     own = true;
                 }
             }
             kept += (own ? 1 : 0) + (nw_ ? 1 : 0);
-            const int po = bk_claim(s_out, lb, own);
+            const unsigned seg = bk_segment(lb, lane);
+            const int ob = 2 * j0 + lb;                      // group bucket of the own output
+            const int po = bk_claim(s_out, ob, own, seg, lane);
             if (own) {
                 if (po < CAP) {
-                    const long long o = (long long)s_b[a][lb] * CAP + po;
+                    const long long o = (long long)s_b[a][ob] * CAP + po;
                     store_key<NW>(OZ, OX, o, skey(a, i));
                     OC[o] = oval;
                 } else {
                     over = true;
                 }
             }
-            const int tb = lb ^ flip;
-            const int pn = bk_claim(s_out, tb, nw_);
+            const int tb = ob ^ flip;                        // the partner bucket of the pair
+            const int pn = bk_claim(s_out, tb, nw_, seg, lane);
             if (nw_) {
                 if (pn < CAP) {
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
@@ -461,45 +523,40 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
             }
         }
         __syncthreads();
-        for (int i = tid; i < TAB; i += T) tab[i] = 0u;     // for the next sub-group
+        uint4 *t4 = reinterpret_cast<uint4 *>(tab);                      // for the next sub-group
+        for (int q = tid; q < TAB / 8; q += T) t4[q] = make_uint4(0u, 0u, 0u, 0u);
+        return j1;
     };
 
-    // ---- prologue: group c in area 0 (copies in flight), group c + grid planned in area 1
+    // ---- prologue: group c staged into area 0 (copies in flight), group c + grid planned in area 1
     long long gi = blockIdx.x;
     load_info(0, gi < ngroups ? gi : -1);
+    load_info(1, gi + gridDim.x < ngroups ? gi + gridDim.x : -1);
     __syncthreads();
     plan(0, 0);
+    plan(1, 0);
     __syncthreads();
     issue(0, 0);
     cp_async_commit();
-    {
-        const long long g1 = gi + gridDim.x;
-        load_info(1, g1 < ngroups ? g1 : -1);
-        __syncthreads();
-        plan(1, 0);
-        __syncthreads();
-    }
     for (int it = 0; gi < ngroups; ++it, gi += gridDim.x) {
         const int a = it & 1;
         const long long gnext = gi + gridDim.x, gafter = gi + 2 * (long long)gridDim.x;
-        // next group's copies (planned last iteration) go in flight now
-        if (gnext < ngroups) issue(a ^ 1, 0);
-        cp_async_commit();
         // the group after next: its pair counts load while this group is processed
         int pb0 = 0, pb1 = 0, pn0 = 0, pn1 = 0;
         if (tid < G && gafter < ngroups) {
             bk_pair(delta, gafter * G + tid, &pb0, &pb1);
             if (pb0 < nb && pb1 < nb) { pn0 = CNT[pb0]; pn1 = CNT[pb1]; }
         }
-        cp_async_wait<1>();
+        cp_async_wait<0>();
         __syncthreads();
+        // the next group's copies (planned last iteration) go in flight now
+        if (gnext < ngroups) issue(a ^ 1, 0);
+        cp_async_commit();
         // this group: its first sub-group is staged in area a, later ones are loaded in turn
         int j0 = 0;
         for (;;) {
-            run(a, s_off[a][2 * (s_j1[a] - j0)]);
-            j0 = s_j1[a];
+            j0 = run(a, j0);
             if (j0 >= G) break;
-            __syncthreads();
             plan(a, j0);
             __syncthreads();
             issue(a, j0);
@@ -508,11 +565,12 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
             __syncthreads();
         }
         // output counts of the group's buckets, then area a takes the group after
-        // next and is planned (warp 0 alone: 2 * G <= 32)
+        // next and is planned (warp 0 alone: 2 * G <= 32); the next iteration's
+        // first barrier publishes both
         if (warp == 0) {
             if (lane < 2 * G) {
                 const int m = s_out[lane];
-                A.cnt[cur ^ 1][s_b[a][lane]] = min(m, CAP);
+                OCNT[s_b[a][lane]] = min(m, CAP);
                 atomicMax(&s_mx, m);
                 s_out[lane] = 0;
             }
@@ -531,7 +589,6 @@ __global__ void __launch_bounds__(BK_THREADS, ITEMS >= 8 ? 1 : BK_MIN_BLOCKS) k_
             __syncwarp();
             plan(a, 0);
         }
-        __syncthreads();
     }
     cp_async_wait<0>();
     // ---- per-rotation totals

@@ -133,6 +133,7 @@ SIGNATURES = {
     "pp_device_info": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
     "pp_debug_fail_alloc": (c_int32, [c_int64]),
     "pp_debug_lookback_timeout": (c_int32, [c_int64]),
+    "pp_debug_bucket_limit": (c_int32, [c_int64]),
 }
 
 

@@ -29,7 +29,7 @@ TUNING_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file
 VARIANTS = [(128, 4), (256, 4), (512, 4), (256, 8), (512, 8), (1024, 8)]
 LOAD_DIVS = (4, 5, 6)
 CHUNKS = (32, 64, 128)
-DEFAULT = (256, 4, 5, 64)
+DEFAULT = (512, 4, 6, 128)
 
 _cache = {}
 

@@ -224,3 +224,91 @@ def test_bucket_config2_whole_circuit():
     z, x, c = v.arrays()
     diag = np.all(x == 0, axis=1)
     assert abs(e - v.expect(0)) <= 1e-12 * max(1e-300, float(np.abs(c[diag]).sum()))
+
+
+@pytest.mark.parametrize("spec,channel", [
+    (("coeff", 1e-6), ("depolarizing", 2e-3)),
+    (("comp", [("coeff", 1e-6), ("weight", 7)]), ("dephasing", 1e-3)),
+])
+@pytest.mark.parametrize("keep_finished", [True, False])
+def test_bucket_batched_instances(spec, channel, keep_finished):
+    """Batched instances on buckets: a 20-qubit chain (39 rotations per layer, so
+    every span between instance ends runs on buckets), uneven depths.  Every
+    instance equals its own oracle run bit for bit (keys, coefficients, final
+    count, <0|O_i|0> within 1e-12 * sum|c_diag|), and the sorted-merge kernels
+    give the same batch bit for bit."""
+    from test_gpu_batch import BIG_APPEND, chain_layer, random_observable
+    nq = 20
+    depths = [1, 3, 4, 0, 2, 5, 3, 4]
+    rng = random.Random(5)
+    gens, acol = chain_layer(nq)
+    obs = [random_observable(rng, nq, 3) for _ in depths]
+    angs = [[rng.uniform(0.05, 0.5), rng.uniform(0.05, 0.5)] for _ in depths]
+    L, D = len(gens), max(depths)
+    assert L >= 32
+
+    def go():
+        return pp.evolve_batch(obs, gens * D, acol * D, angs, [d * L for d in depths], nq=nq,
+                               truncation=strategy(spec), channel=(channel[0], channel[1], None),
+                               channel_every=L, keep_finished=keep_finished)
+
+    res = _on("buckets", go)
+    til = _on("tiles", go)
+    assert res.stats["bucket_rot"] > 0 and til.stats["bucket_rot"] == 0
+    assert np.array_equal(res.n_final, til.n_final)
+    assert np.array_equal(res.expect.view(np.uint64), til.expect.view(np.uint64))
+    if keep_finished:
+        parts = pp.split_instances(*res.vector.to_arrays(), len(depths))
+        tparts = pp.split_instances(*til.vector.to_arrays(), len(depths))
+    for i, d in enumerate(depths):
+        v = orc.OracleSPV(nq, max(16, 2 * len(obs[i])), BIG_APPEND)
+        v.upload([t[0] for t in obs[i]], [t[1] for t in obs[i]], [t[2] for t in obs[i]])
+        for _ in range(d):
+            v.evolve(gens, [angs[i][a] for a in acol], window=1, strict=filt(spec))
+            v.channel(CHANNEL_KIND[channel[0]], [channel[1]])
+        oz, ox, oc = v.arrays()
+        assert res.n_final[i] == len(v)
+        diag = ox[:, 0] == 0
+        assert abs(res.expect[i] - v.expect(0)) <= 1e-12 * max(1e-300, float(np.abs(oc[diag]).sum()))
+        if keep_finished:
+            gz, gx, gc = parts[i]
+            assert np.array_equal(gz, oz[:, 0]) and np.array_equal(gx, ox[:, 0]), f"instance {i}: key sets differ"
+            assert np.array_equal(gc.view(np.uint64), oc.view(np.uint64)), f"instance {i}: coefficients differ"
+            for a, b in zip(parts[i], tparts[i]):
+                assert np.array_equal(np.asarray(a).view(np.uint64), np.asarray(b).view(np.uint64))
+    if keep_finished:
+        pp.check_spv(res.vector)
+
+
+@pytest.mark.parametrize("limit", [1 << 21, 1 << 12])
+def test_bucket_layout_too_large_hands_over(limit):
+    """When the next bucket layout does not fit in device memory (here: a test cap
+    on its slots), the rotations done so far go back to the dense sorted set and
+    the sorted-merge kernels finish the sequence -- in the middle of the call
+    (2^21 slots: the set outgrows it) or from the start (2^12 slots: nothing
+    fits).  Same vector as the oracle's, bit for bit, either way."""
+    rng = random.Random(64)
+    N = 64
+    terms = rand_terms(rng, N, 600)          # grows to 1.7e6 terms
+    gens, angs = [], []
+    for _ in range(40):
+        i, j = rng.sample(range(12), 2)
+        gens.append(((1 << i) | (1 << j), 0) if rng.random() < 0.6 else (0, 1 << i))
+        angs.append(rng.uniform(0.2, 1.2))
+    spec = ("coeff", 1e-3)
+    v = _oracle(N, terms)
+    g = _gpu(v, N)
+    v.evolve(gens, angs, window=1, strict=filt(spec))
+    st = {}
+    _lib.check(_lib.lib.pp_debug_bucket_limit(limit))
+    try:
+        _on("buckets", lambda: pp.evolve_(g, [pp.PauliBasis(N, a, b) for a, b in gens], angs,
+                                          truncation=strategy(spec), stats=st))
+    finally:
+        _lib.check(_lib.lib.pp_debug_bucket_limit(0))
+    assert len(v) > 10**6
+    if limit > 1 << 12:
+        assert 0 < st["bucket_rot"] < len(gens)
+    else:
+        assert st["bucket_rot"] == 0
+    _same(g, v)
