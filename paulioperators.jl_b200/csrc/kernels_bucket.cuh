@@ -149,16 +149,25 @@ __device__ __forceinline__ unsigned bk_segment(int lb, int lane) {
     return (above ? (1u << (__ffs(above) - 1)) - 1u : 0xffffffffu) & ~((1u << s0) - 1u);
 }
 
-// Position in output bucket ob for every lane that passes `want` (ob is the same
-// across a segment): the segment's first wanting lane takes consecutive slots
-// for all of them from one shared-memory atomic.
-__device__ __forceinline__ int bk_claim(int *s_out, int ob, bool want, unsigned seg, int lane) {
-    const unsigned peers = __ballot_sync(0xffffffffu, want) & seg;
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (want && lane == leader) base = atomicAdd(&s_out[ob], __popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader < 0 ? lane : leader);
-    return want ? base + __popc(peers & ((1u << lane) - 1u)) : -1;
+// Output slots of a run of lanes (seg) that share their local bucket ob: `own`
+// lanes append to bucket ob, `nw` lanes (new sin branches) to the partner bucket
+// tb = ob ^ flip.  Both buckets belong to pair ob / 2, whose two counters are
+// packed in one 64-bit word (bucket 2j low, 2j + 1 high), so the run's first
+// claiming lane takes the slots of every claim of the run with one atomic.
+// When tb == ob the new terms follow the run's own outputs.
+__device__ __forceinline__ void bk_claim2(unsigned long long *s_out2, int ob, int tb, bool own, bool nw,
+                                          unsigned seg, int lane, int *po, int *pn) {
+    const unsigned w1 = __ballot_sync(0xffffffffu, own) & seg, w2 = __ballot_sync(0xffffffffu, nw) & seg;
+    const int c1 = __popc(w1), c2 = __popc(w2);
+    const int leader = __ffs(w1 | w2) - 1;
+    const int so = 32 * (ob & 1), sn = 32 * (tb & 1);
+    unsigned long long old = 0;
+    if (lane == leader && leader >= 0)
+        old = atomicAdd(&s_out2[ob >> 1], ((unsigned long long)c1 << so) + ((unsigned long long)c2 << sn));
+    old = __shfl_sync(0xffffffffu, old, leader < 0 ? lane : leader);
+    const unsigned lt = (1u << lane) - 1u;
+    *po = (int)(unsigned)(old >> so) + __popc(w1 & lt);
+    *pn = (int)(unsigned)(old >> sn) + (tb == ob ? c1 : 0) + __popc(w2 & lt);
 }
 
 // The common criteria of a compiled filter in registers (coefficient
@@ -250,7 +259,8 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     __shared__ GenRec g;
     __shared__ unsigned s_delta;
     __shared__ int s_b[2][NBK], s_n[2][NBK], s_off[2][NBK + 1], s_j1[2];
-    __shared__ int s_out[NBK], s_mx, s_bad;
+    __shared__ unsigned long long s_out2[GMAX];   // output counts of pair j: bucket 2j low, 2j + 1 high
+    __shared__ int s_mx, s_bad;
     __shared__ int s_red[3][T / 32];
     extern __shared__ u64 bsm[];
     // staging area a: keys (NW words each, z then x), coefficients; then the key
@@ -290,7 +300,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         uint4 *t4 = reinterpret_cast<uint4 *>(tab);
         for (int i = tid; i < TAB / 8; i += T) t4[i] = make_uint4(0u, 0u, 0u, 0u);
     }
-    if (tid < NBK) s_out[tid] = 0;
+    if (tid < GMAX) s_out2[tid] = 0ull;
     __syncthreads();
     const unsigned delta = s_delta;
     const long long nb = 1ll << A.bits;
@@ -337,19 +347,29 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             s_n[a][2 * tid] = n0; s_n[a][2 * tid + 1] = n1;
         }
     };
-    // first sub-group [j0, j1) of pairs from j0 that fits the staging area; offsets (thread 0)
+    // first sub-group [j0, j1) of pairs from j0 that fits the staging area, and its
+    // offsets: a prefix sum over the pairs in warp 0 (G <= 16 pairs, one per lane;
+    // called by warp 0 only).  A single pair always fits (counts are at most CAP).
     auto plan = [&](int a, int j0) {
-        if (tid == 0) {
-            int j = j0, tot = 0;
-            while (j < G && tot + s_n[a][2 * j] + s_n[a][2 * j + 1] <= SMI) {
-                s_off[a][2 * (j - j0)] = tot;
-                tot += s_n[a][2 * j];
-                s_off[a][2 * (j - j0) + 1] = tot;
-                tot += s_n[a][2 * j + 1];
-                ++j;
-            }
-            s_off[a][2 * (j - j0)] = tot;
-            s_j1[a] = j;
+        const int j = j0 + lane;
+        const int n0 = j < G ? s_n[a][2 * j] : 0, n1 = j < G ? s_n[a][2 * j + 1] : 0;
+        int inc = n0 + n1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += y;
+        }
+        const int exc = inc - n0 - n1;
+        const bool fits = j < G && (inc <= SMI || lane == 0);
+        const int cnt = __popc(__ballot_sync(0xffffffffu, fits));       // fits is a prefix of the lanes
+        if (fits) {
+            s_off[a][2 * lane] = exc;
+            s_off[a][2 * lane + 1] = exc + n0;
+        }
+        const int tot = __shfl_sync(0xffffffffu, inc, max(cnt, 1) - 1);
+        if (lane == 0) {
+            s_off[a][2 * cnt] = tot;
+            s_j1[a] = j0 + cnt;
         }
     };
     // copies of the planned sub-group's terms into area a (asynchronous)
@@ -496,8 +516,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             }
             kept += (own ? 1 : 0) + (nw_ ? 1 : 0);
             const unsigned seg = bk_segment(lb, lane);
-            const int ob = 2 * j0 + lb;                      // group bucket of the own output
-            const int po = bk_claim(s_out, ob, own, seg, lane);
+            const int ob = 2 * j0 + (lb & 0x3f);             // group bucket of the own output
+            const int tb = ob ^ flip;                        // the partner bucket of the pair
+            int po, pn;
+            bk_claim2(s_out2, ob, tb, own, nw_, seg, lane, &po, &pn);
             if (own) {
                 if (po < CAP) {
                     const long long o = (long long)s_b[a][ob] * CAP + po;
@@ -507,8 +529,6 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     over = true;
                 }
             }
-            const int tb = ob ^ flip;                        // the partner bucket of the pair
-            const int pn = bk_claim(s_out, tb, nw_, seg, lane);
             if (nw_) {
                 if (pn < CAP) {
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
@@ -533,8 +553,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     load_info(0, gi < ngroups ? gi : -1);
     load_info(1, gi + gridDim.x < ngroups ? gi + gridDim.x : -1);
     __syncthreads();
-    plan(0, 0);
-    plan(1, 0);
+    if (warp == 0) {
+        plan(0, 0);
+        plan(1, 0);
+    }
     __syncthreads();
     issue(0, 0);
     cp_async_commit();
@@ -557,7 +579,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         for (;;) {
             j0 = run(a, j0);
             if (j0 >= G) break;
-            plan(a, j0);
+            if (warp == 0) plan(a, j0);
             __syncthreads();
             issue(a, j0);
             cp_async_commit();
@@ -569,12 +591,12 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         // first barrier publishes both
         if (warp == 0) {
             if (lane < 2 * G) {
-                const int m = s_out[lane];
+                const int m = (int)(unsigned)(s_out2[lane >> 1] >> (32 * (lane & 1)));
                 OCNT[s_b[a][lane]] = min(m, CAP);
                 atomicMax(&s_mx, m);
-                s_out[lane] = 0;
             }
             __syncwarp();
+            if (lane < G) s_out2[lane] = 0ull;
             if (lane < G) {
                 if (gafter < ngroups) {
                     if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
