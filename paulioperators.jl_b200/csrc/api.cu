@@ -36,6 +36,23 @@ static int fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
 }
+
+// PAULIPROP_TRACE=1: one line on stderr per engine transition (bucketed spans,
+// splits, hand-overs to the sorted-merge kernels, growth of the live sets).
+static bool trace_on() {
+    static const bool on = [] {
+        const char *e = getenv("PAULIPROP_TRACE");
+        return e && *e && strcmp(e, "0") != 0;
+    }();
+    return on;
+}
+#define PP_TRACE(...)                                   \
+    do {                                                \
+        if (trace_on()) {                               \
+            fprintf(stderr, "[pauliprop] " __VA_ARGS__); \
+            fputc('\n', stderr);                        \
+        }                                               \
+    } while (0)
 extern "C" const char *pp_last_error(void) { return g_err.c_str(); }
 int pp_fail_msg(int code, const char *msg) { return fail(code, msg); }
 
@@ -258,8 +275,9 @@ static int ensure_dense(pp_spv *h) {
 // preserving the live terms (copied into set 0).
 // With preserve == false the live terms are not copied (the caller refills the
 // sets) and the state's live count becomes 0 once the new sets are in place.
-static int grow_live(pp_spv *h, long long need, bool preserve = true) {
-    long long newcap = std::max(need, std::max(2 * h->cap, (long long)4096));
+// want: a larger capacity to prefer (growth ahead of time); only need is required.
+static int grow_live(pp_spv *h, long long need, bool preserve = true, long long want = 0) {
+    long long newcap = std::max(std::max(need, want), std::max(2 * h->cap, (long long)4096));
     if (newcap > 0x7fffffffll - 8192) newcap = std::max(need, 0x7fffffffll - 8192);
     if (need > 0x7fffffffll - 8192) return fail(PP_OUT_OF_MEMORY, "term count exceeds 2^31 - 8192");
     DevState st;
@@ -268,16 +286,20 @@ static int grow_live(pp_spv *h, long long need, bool preserve = true) {
         TRY(ensure_dense(h));
         TRY(read_state(h, &st));
     }
-    // refuse a growth that would leave less than 4 GiB of device memory free
+    // refuse a growth that would leave less than 4 GiB of device memory free; when
+    // the doubled capacity does not fit, step down towards the capacity needed
     {
         size_t freeb = 0, totalb = 0;
         if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) {
-            const double want = (double)newcap * (2.0 * (2 * h->NW * 8 + 8) + 12.0 + 4.0 * TAU_MAX * 2.0 / SEG);
-            if (want + 4.0 * (1ull << 30) > (double)freeb)
+            const double per = 2.0 * (2 * h->NW * 8 + 8) + 12.0 + 4.0 * TAU_MAX * 2.0 / SEG;
+            const double room = (double)freeb - 4.0 * (1ull << 30);
+            while ((double)newcap * per > room && newcap > need) newcap = std::max(need, newcap - newcap / 4);
+            if ((double)newcap * per > room)
                 return fail(PP_OUT_OF_MEMORY, "growing to " + std::to_string(newcap) +
                                                   " terms would leave less than 4 GiB of device memory free");
         }
     }
+    PP_TRACE("grow live sets: need %lld, capacity %lld -> %lld", need, h->cap, newcap);
     // every new buffer first; on failure the handle is unchanged
     u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
     double *nc[2] = {nullptr, nullptr};
@@ -337,9 +359,9 @@ static int grow_live(pp_spv *h, long long need, bool preserve = true) {
     return PP_OK;
 }
 
-static int ensure_live(pp_spv *h, long long need, bool preserve = true) {
+static int ensure_live(pp_spv *h, long long need, bool preserve = true, long long want = 0) {
     if (need <= h->cap) return PP_OK;
-    return grow_live(h, need, preserve);
+    return grow_live(h, need, preserve, want);
 }
 
 // General path: physical append buffers (keeping pending appends) and sort temps.
@@ -861,7 +883,19 @@ static void bk_launch(pp_spv *h, const BkVariant *v, const BkArgs &A, int k) {
     const bool batch = NW == 2 && h->batch_on;
     const int occ = NW == 1 ? oc.occ1 : batch ? oc.occb : oc.occ2;
     const int grid = (int)std::min(pairs, (long long)h->nsm * occ);
-    (NW == 1 ? v->k1 : batch ? v->kb : v->k2)<<<grid, BK_THREADS, NW == 1 ? v->smem1 : v->smem2, h->stream>>>(A, k);
+    // programmatic dependent launch: the rotation's prologue overlaps the previous
+    // rotation's tail (k_bk_rotate waits for its outputs in griddepcontrol.wait)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(BK_THREADS);
+    cfg.dynamicSmemBytes = NW == 1 ? v->smem1 : v->smem2;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, NW == 1 ? v->k1 : batch ? v->kb : v->k2, A, k);
 }
 
 // Hash rows: fixed pseudo-random words (splitmix64 from a fixed seed), so the
@@ -964,20 +998,22 @@ static int bk_reserve(pp_spv *h, int bits, int *cur, int cur_bits) {
     if (cur_bits >= 0 && h->bk_cap != h->tune.bucket_cap)
         return fail(PP_ERROR_EXCEPTION, "internal error: bucket capacity changed inside a call");
     const int cap = h->tune.bucket_cap;
-    const int nbits = std::min(BK_ROWS, std::max(bits + 1, h->bk_cap == cap ? h->bk_bits_cap : 0));
-    const long long slots = (long long)cap << nbits;
-    {
-        // the two bucket sets, and room to convert a full layout (at most slots / 2
-        // terms before the next split) back to a dense sorted set, plus 4 GiB
+    // the two bucket sets, and room to convert a full layout (at most slots / 2
+    // terms before the next split) back to a dense sorted set, plus 4 GiB; one
+    // split of headroom (2^(bits+1) buckets) when that fits, else 2^bits
+    auto fits = [&](long long sl) {
         size_t freeb = 0, totalb = 0;
         if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) {
             const double B = 16.0 * NW + 8.0;
-            const double want = 2.0 * (double)slots * B + 1.5 * (double)slots * B;
-            if (want + 4.0 * (1ull << 30) > (double)freeb) return BK_NOFIT;
+            if (3.5 * (double)sl * B + 4.0 * (1ull << 30) > (double)freeb) return false;
         }
         const long long lim = g_bk_slot_limit.load();
-        if (lim > 0 && slots > lim) return BK_NOFIT;
-    }
+        return !(lim > 0 && sl > lim);
+    };
+    int nbits = std::min(BK_ROWS, std::max(bits + 1, h->bk_cap == cap ? h->bk_bits_cap : 0));
+    if (!fits((long long)cap << nbits)) nbits = bits;
+    if (!fits((long long)cap << nbits)) return BK_NOFIT;
+    const long long slots = (long long)cap << nbits;
     u64 *nz[2] = {nullptr, nullptr}, *nx[2] = {nullptr, nullptr};
     double *nc[2] = {nullptr, nullptr};
     int *nn[2] = {nullptr, nullptr};
@@ -1087,6 +1123,7 @@ static int bk_to_dense(pp_spv *h, int cur, int bits) {
     long long n = 0;
     CU(cudaMemcpyAsync(&n, h->bk_off + nb, sizeof n, cudaMemcpyDeviceToHost, s));
     TRY(sync_check(h));
+    PP_TRACE("buckets -> dense: %lld terms (2^%d buckets)", n, bits);
     TRY(radix_reserve(h, n));
     TRY(ensure_live(h, n + 1, false));
     k_bk_gather<NW><<<std::max(1, std::min(h->nsm * 8, (nb + 7) / 8)), 256, 0, s>>>(
@@ -1133,12 +1170,24 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
     }
     // bucket the live set
     int bits = bk_bits_for(n0, h->tune.bucket_cap, h->tune.load_div), cur = 0;
+    PP_TRACE("buckets: rotations [%lld, %lld), %lld live terms, 2^%d buckets of %d", start, L, n0, bits,
+             h->tune.bucket_cap);
+    // (when that layout does not fit, fewer and fuller buckets down to a mean load
+    // of cap / 3, as long as no bucket is more than half full)
+    const int bmin = bk_bits_for(n0, h->tune.bucket_cap, 3);
+    bool lowered = false;
     for (;;) {
         const int rr = bk_reserve<NW>(h, bits, &cur, -1);
+        if (rr == BK_NOFIT && bits > bmin) {
+            --bits;
+            lowered = true;
+            continue;
+        }
         if (rr) return rr;                  // BK_NOFIT: nothing changed, the dense set is the input
         int mx = 0;
         TRY(bk_scatter<NW>(h, h->z[st.cur], h->x[st.cur], h->c[st.cur], n0, -1, 0, 0, bits, &mx));
         if (mx >= 0 && mx <= h->bk_cap / 2) break;
+        if (lowered) return BK_NOFIT;       // the fuller layout fails the half-full rule, a larger one does not fit
         if (++bits > BK_ROWS) return fail(PP_OUT_OF_MEMORY, "bucketed live set exceeds 2^26 buckets");
     }
     cudaStream_t s = h->stream;
@@ -1267,6 +1316,8 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
         }
         if (done < L && (over || last.maxcnt > h->bk_cap / 2)) {
             const int rr = bk_regrid<NW>(h, &cur, &bits);
+            PP_TRACE("buckets: split at rotation %lld (largest bucket %d) -> 2^%d buckets%s", done, last.maxcnt, bits,
+                     rr == BK_NOFIT ? ": does not fit, hand-over to the sorted-merge kernels" : "");
             if (rr == BK_NOFIT) {
                 // no room for a larger layout: the rotations so far go back to the
                 // dense sorted set, the bucket sets are freed, and the sorted-merge
@@ -1329,6 +1380,8 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
         if (use_bk && L - done >= BK_MIN_ROT) {
             const int rb = run_bucket<NW>(h, done, L, ctr, prof, per_rot);
             if (rb != BK_NOFIT) return rb;
+            bk_release(h);                  // their memory goes to the sorted-merge kernels
+            PP_TRACE("buckets do not fit at rotation %lld: sorted-merge kernels for the rest of the call", done);
             // no room for buckets: the rest of the sequence on the sorted-merge kernels,
             // from the rotation the bucketed part reached
             use_bk = false;
@@ -1416,8 +1469,9 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
         if (st.err) { ensure_dense(h); return check_err(h, st); }
         done = st.rot;
         // grow ahead of time: the merge's per-tile output slots need ~1.25 (n + a) <= 2.5 n
+        // (3 n required, 6 n preferred while device memory allows)
         if (done < L && 3 * st.n > h->cap) {
-            TRY(ensure_live(h, 6 * st.n));
+            TRY(ensure_live(h, 3 * st.n, true, 6 * st.n));
             table = false;
         }
     }

@@ -126,18 +126,6 @@ __host__ __device__ constexpr int bk_group_max() {
     return 4 * BK_THREADS * ITEMS / CAP < 16 ? 4 * BK_THREADS * ITEMS / CAP : 16;
 }
 
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 // Lanes of the warp whose local bucket equals this lane's: the staged terms of a
 // group lie in bucket order, so equal buckets form one run of consecutive lanes.
 __device__ __forceinline__ unsigned bk_segment(int lb, int lane) {
@@ -149,25 +137,17 @@ __device__ __forceinline__ unsigned bk_segment(int lb, int lane) {
     return (above ? (1u << (__ffs(above) - 1)) - 1u : 0xffffffffu) & ~((1u << s0) - 1u);
 }
 
-// Output slots of a run of lanes (seg) that share their local bucket ob: `own`
-// lanes append to bucket ob, `nw` lanes (new sin branches) to the partner bucket
-// tb = ob ^ flip.  Both buckets belong to pair ob / 2, whose two counters are
-// packed in one 64-bit word (bucket 2j low, 2j + 1 high), so the run's first
-// claiming lane takes the slots of every claim of the run with one atomic.
-// When tb == ob the new terms follow the run's own outputs.
-__device__ __forceinline__ void bk_claim2(unsigned long long *s_out2, int ob, int tb, bool own, bool nw,
-                                          unsigned seg, int lane, int *po, int *pn) {
-    const unsigned w1 = __ballot_sync(0xffffffffu, own) & seg, w2 = __ballot_sync(0xffffffffu, nw) & seg;
-    const int c1 = __popc(w1), c2 = __popc(w2);
-    const int leader = __ffs(w1 | w2) - 1;
-    const int so = 32 * (ob & 1), sn = 32 * (tb & 1);
-    unsigned long long old = 0;
-    if (lane == leader && leader >= 0)
-        old = atomicAdd(&s_out2[ob >> 1], ((unsigned long long)c1 << so) + ((unsigned long long)c2 << sn));
-    old = __shfl_sync(0xffffffffu, old, leader < 0 ? lane : leader);
-    const unsigned lt = (1u << lane) - 1u;
-    *po = (int)(unsigned)(old >> so) + __popc(w1 & lt);
-    *pn = (int)(unsigned)(old >> sn) + (tb == ob ? c1 : 0) + __popc(w2 & lt);
+// Position in output bucket ob for every lane that passes `want` (ob is the same
+// across a segment): the segment's first wanting lane takes consecutive slots
+// for all of them from one shared-memory atomic.  (Packing a pair's two counters
+// into one 64-bit atomic for both claims of a round measured 5 % slower.)
+__device__ __forceinline__ int bk_claim(int *s_out, int ob, bool want, unsigned seg, int lane) {
+    const unsigned peers = __ballot_sync(0xffffffffu, want) & seg;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (want && lane == leader) base = atomicAdd(&s_out[ob], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader < 0 ? lane : leader);
+    return want ? base + __popc(peers & ((1u << lane) - 1u)) : -1;
 }
 
 // The common criteria of a compiled filter in registers (coefficient
@@ -248,21 +228,22 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     static_assert(SMI < 0x10000, "16-bit key index entries");
     static_assert(!BATCH || NW == 2, "batched instances use two-word keys");
     DevState *S = A.S;
-    // one read of the error word for the whole CTA (another CTA may set it meanwhile)
+    // Launched as a programmatic dependent of the previous rotation: the next
+    // rotation's CTAs may start as this one's finish.  Everything before
+    // griddepcontrol.wait reads only what no rotation writes (the cursor set
+    // before the graph launch, the generator, the hash rows).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     __shared__ int s_err;
-    if (threadIdx.x == 0) s_err = S->err;
-    __syncthreads();
-    if (s_err) return;
     const long long r = S->bk_rot0 + k;
     if (r >= S->rot_end) return;
     const int cur = (S->bk_cur0 + k) & 1;
     __shared__ GenRec g;
     __shared__ unsigned s_delta;
     __shared__ int s_b[2][NBK], s_n[2][NBK], s_off[2][NBK + 1], s_j1[2];
-    __shared__ unsigned long long s_out2[GMAX];   // output counts of pair j: bucket 2j low, 2j + 1 high
-    __shared__ int s_mx, s_bad;
+    __shared__ int s_out[NBK], s_mx, s_bad;
     __shared__ int s_red[3][T / 32];
-    extern __shared__ u64 bsm[];
+    __shared__ __align__(8) unsigned long long s_mbar[2];   // completion of each staging area's copies
+    extern __shared__ __align__(128) u64 bsm[];
     // staging area a: keys (NW words each, z then x), coefficients; then the key
     // index and, per area, each staged term's local bucket (bit 7: dropped by the
     // early merge)
@@ -278,11 +259,25 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         s_delta = bk_hash<NW>(g.gz, g.gx, A.rows, A.bits);
         s_bad = 0;
         s_mx = 0;
+        mbar_init(smem_addr(&s_mbar[0]), 1);
+        mbar_init(smem_addr(&s_mbar[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (r + 1 >= A.rec_len) {
         if (tid == 0) flag_bounds(S, 2, r);
         return;
     }
+    {
+        uint4 *t4 = reinterpret_cast<uint4 *>(tab);
+        for (int i = tid; i < TAB / 8; i += T) t4[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (tid < NBK) s_out[tid] = 0;
+    // the previous rotation's outputs (and error word) are visible from here on;
+    // one read of the error word for the whole CTA (another CTA may set it meanwhile)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (tid == 0) s_err = S->err;
+    __syncthreads();
+    if (s_err) return;
     // the state entering this rotation, from the previous rotation's record (the
     // early-merge rule of spv_evolve.jl:356-362)
     const BkRec &prev = A.rec[r];
@@ -296,12 +291,6 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         me.acap = acap;
         me.pref = pref ? 1 : 0;
     }
-    {
-        uint4 *t4 = reinterpret_cast<uint4 *>(tab);
-        for (int i = tid; i < TAB / 8; i += T) t4[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    if (tid < GMAX) s_out2[tid] = 0ull;
-    __syncthreads();
     const unsigned delta = s_delta;
     const long long nb = 1ll << A.bits;
     const long long pairs = nb / 2;
@@ -349,10 +338,14 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     };
     // first sub-group [j0, j1) of pairs from j0 that fits the staging area, and its
     // offsets: a prefix sum over the pairs in warp 0 (G <= 16 pairs, one per lane;
-    // called by warp 0 only).  A single pair always fits (counts are at most CAP).
+    // called by warp 0 only).  Each bucket's run is padded to an even length, so
+    // every run starts 16-byte aligned for the bulk copies.  A single pair always
+    // fits (counts are at most CAP, which is even).
     auto plan = [&](int a, int j0) {
         const int j = j0 + lane;
-        const int n0 = j < G ? s_n[a][2 * j] : 0, n1 = j < G ? s_n[a][2 * j + 1] : 0;
+        int n0 = j < G ? s_n[a][2 * j] : 0, n1 = j < G ? s_n[a][2 * j + 1] : 0;
+        n0 += n0 & 1;
+        n1 += n1 & 1;
         int inc = n0 + n1;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -372,38 +365,49 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             s_j1[a] = j0 + cnt;
         }
     };
-    // copies of the planned sub-group's terms into area a (asynchronous)
+    // copies of the planned sub-group's terms into area a (asynchronous): one lane
+    // of warp 0 per bucket issues bulk copies of its run of keys and coefficients,
+    // each lane announcing its bytes on the area's mbarrier before copying, and
+    // lane 0 arrives once all lanes have; every warp writes the local-bucket byte of
+    // each staged slot (bit 7 on a run's padding slot).  Every call arrives on the
+    // mbarrier exactly once, so the wait for it always ends.
     auto issue = [&](int a, int j0) {
         const int nloc = 2 * (s_j1[a] - j0);
         const int ntot = s_off[a][nloc];
         unsigned char *sbk = sbk0 + a * SMI;
-        if (ntot > SMI || nloc > NBK) {      // the planner never builds such a sub-group
-            if (tid == 0) flag_bounds(S, 5, ((long long)ntot << 16) | nloc);
-            return;
-        }
-        // warp w copies buckets w, w + 8, ... (each a contiguous run of slots)
-        for (int lb = warp; lb < nloc; lb += T / 32) {
-            const int bq = s_b[a][2 * j0 + lb];
-            const int o0 = s_off[a][lb], cnt = s_off[a][lb + 1] - o0;
-            if (bq < 0 || bq >= nb || cnt < 0 || cnt > CAP) {
-                if (lane == 0) flag_bounds(S, 6, ((long long)bq << 20) | (cnt & 0xfffff));
-                for (int t = lane; t < cnt; t += 32) sbk[o0 + t] = (unsigned char)lb;
-                continue;
-            }
-            for (int t = lane; t < cnt; t += 32) {
-                const int i = o0 + t;
-                const long long p = (long long)bq * CAP + t;
-                if constexpr (NW == 1) {
-                    cp_async8(skz(a) + i, Z + p);
-                    cp_async8(skx(a) + i, X + p);
-                } else {
-                    cp_async16(skz(a) + 2 * i, Z + 2 * p);
-                    cp_async16(skx(a) + 2 * i, X + 2 * p);
+        const bool bad = ntot > SMI || nloc > NBK;       // the planner never builds such a sub-group
+        const uint32_t mb = smem_addr(&s_mbar[a]);
+        if (warp == 0) {
+            if (bad && lane == 0) flag_bounds(S, 5, ((long long)ntot << 16) | nloc);
+            if (!bad && lane < nloc) {
+                const int bq = s_b[a][2 * j0 + lane];
+                const int o0 = s_off[a][lane], len = s_off[a][lane + 1] - o0;
+                if (bq < 0 || bq >= nb || len < 0 || len > CAP || (o0 & 1)) {
+                    flag_bounds(S, 6, ((long long)bq << 20) | (len & 0xfffff));
+                } else if (len > 0) {
+                    const long long p = (long long)bq * CAP;
+                    mbar_expect_tx(mb, (uint32_t)len * (uint32_t)(2 * NW * 8 + 8));
+                    fence_async_smem();
+                    bulk_g2s(smem_addr(skz(a) + NW * o0), Z + NW * p, (uint32_t)(len * NW * 8), mb);
+                    bulk_g2s(smem_addr(skx(a) + NW * o0), X + NW * p, (uint32_t)(len * NW * 8), mb);
+                    bulk_g2s(smem_addr(sc(a) + o0), C + p, (uint32_t)(len * 8), mb);
                 }
-                cp_async8(sc(a) + i, C + p);
-                sbk[i] = (unsigned char)lb;
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(mb);
         }
+        if (bad) return;
+        for (int lb = warp; lb < nloc; lb += T / 32) {
+            const int o0 = s_off[a][lb], len = s_off[a][lb + 1] - o0, cnt = s_n[a][2 * j0 + lb];
+            for (int t = lane; t < len; t += 32) sbk[o0 + t] = (unsigned char)(t < cnt ? lb : (0x80 | lb));
+        }
+    };
+    unsigned phase = 0;                      // bit a: parity of area a's next mbarrier phase
+    auto staged = [&](int a) {               // wait for area a's copies (bounded)
+        if (!mbar_wait(smem_addr(&s_mbar[a]), (phase >> a) & 1u)) {
+            if (tid == 0) atomicOr(&S->err, ERR_TIMEOUT);
+        }
+        phase ^= 1u << a;
     };
     int cre = 0, alive = 0, kept = 0;
     bool over = false;
@@ -428,6 +432,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         // anticommute with G: only they can be a partner (P xor G anticommutes
         // exactly when P does), and a dropped partner counts as absent
         for (int i = tid; i < ntot; i += T) {
+            if (sbk[i] & 0x80) continue;     // a run's padding slot
             const Key<NW> kk = skey(a, i);
             if (pref && drop_q<NW>(fs, P.strict, kk, fabs(sc(a)[i]))) {
                 sbk[i] |= 0x80;
@@ -516,10 +521,8 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             }
             kept += (own ? 1 : 0) + (nw_ ? 1 : 0);
             const unsigned seg = bk_segment(lb, lane);
-            const int ob = 2 * j0 + (lb & 0x3f);             // group bucket of the own output
-            const int tb = ob ^ flip;                        // the partner bucket of the pair
-            int po, pn;
-            bk_claim2(s_out2, ob, tb, own, nw_, seg, lane, &po, &pn);
+            const int ob = 2 * j0 + lb;                      // group bucket of the own output
+            const int po = bk_claim(s_out, ob, own, seg, lane);
             if (own) {
                 if (po < CAP) {
                     const long long o = (long long)s_b[a][ob] * CAP + po;
@@ -529,6 +532,8 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     over = true;
                 }
             }
+            const int tb = ob ^ flip;                        // the partner bucket of the pair
+            const int pn = bk_claim(s_out, tb, nw_, seg, lane);
             if (nw_) {
                 if (pn < CAP) {
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
@@ -558,8 +563,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         plan(1, 0);
     }
     __syncthreads();
-    issue(0, 0);
-    cp_async_commit();
+    if (gi < ngroups) issue(0, 0);
     for (int it = 0; gi < ngroups; ++it, gi += gridDim.x) {
         const int a = it & 1;
         const long long gnext = gi + gridDim.x, gafter = gi + 2 * (long long)gridDim.x;
@@ -569,11 +573,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             bk_pair(delta, gafter * G + tid, &pb0, &pb1);
             if (pb0 < nb && pb1 < nb) { pn0 = CNT[pb0]; pn1 = CNT[pb1]; }
         }
-        cp_async_wait<0>();
+        staged(a);
         __syncthreads();
         // the next group's copies (planned last iteration) go in flight now
         if (gnext < ngroups) issue(a ^ 1, 0);
-        cp_async_commit();
         // this group: its first sub-group is staged in area a, later ones are loaded in turn
         int j0 = 0;
         for (;;) {
@@ -582,8 +585,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             if (warp == 0) plan(a, j0);
             __syncthreads();
             issue(a, j0);
-            cp_async_commit();
-            cp_async_wait<0>();
+            staged(a);
             __syncthreads();
         }
         // output counts of the group's buckets, then area a takes the group after
@@ -591,12 +593,12 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         // first barrier publishes both
         if (warp == 0) {
             if (lane < 2 * G) {
-                const int m = (int)(unsigned)(s_out2[lane >> 1] >> (32 * (lane & 1)));
+                const int m = s_out[lane];
                 OCNT[s_b[a][lane]] = min(m, CAP);
                 atomicMax(&s_mx, m);
+                s_out[lane] = 0;
             }
             __syncwarp();
-            if (lane < G) s_out2[lane] = 0ull;
             if (lane < G) {
                 if (gafter < ngroups) {
                     if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
@@ -612,7 +614,6 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             plan(a, 0);
         }
     }
-    cp_async_wait<0>();
     // ---- per-rotation totals
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {

@@ -191,14 +191,14 @@ def PauliSum_from(v):
 def _gen_words(N, generators):
     nw = nwords(N)
     L = len(generators)
-    gz = np.zeros((L, nw), dtype=np.uint64)
-    gx = np.zeros((L, nw), dtype=np.uint64)
     m = (1 << 64) - 1
-    for i, g in enumerate(generators):
-        z, x = (g.z, g.x) if isinstance(g, PauliBasis) else (int(g[0]), int(g[1]))
-        for w in range(nw):
-            gz[i, w] = (z >> (64 * w)) & m
-            gx[i, w] = (x >> (64 * w)) & m
+    zs = [g.z if isinstance(g, PauliBasis) else int(g[0]) for g in generators]
+    xs = [g.x if isinstance(g, PauliBasis) else int(g[1]) for g in generators]
+    gz = np.empty((L, nw), dtype=np.uint64)
+    gx = np.empty((L, nw), dtype=np.uint64)
+    for w in range(nw):
+        gz[:, w] = np.fromiter(((z >> (64 * w)) & m for z in zs), dtype=np.uint64, count=L)
+        gx[:, w] = np.fromiter(((x >> (64 * w)) & m for x in xs), dtype=np.uint64, count=L)
     return gz, gx
 
 
