@@ -411,7 +411,17 @@ def run_ours_batch(args):
     rp = one_step(profile=True)
     sp = rp.stats
     B = BYTES_PER_TERM[2]
-    achieved = B * (sp["merge_in"] + sp["merge_out"]) / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
+    if sp["bucket_rot"] > 0:
+        # rotations on buckets: B*(n_in + n_out) per k_bk_rotate launch over the timed
+        # graph replays (t_merge also holds any span that ran on the sorted-merge kernels)
+        dom_bytes = sp["bucket_bytes"]
+        tune = pp.tune.get_tuning(v)
+        dom_kernel = (f"k_bk_rotate<2,{tune[0]},{tune[1]},batched> (rotation + partner merge + filter over "
+                      f"bucket pairs, 40-byte instance-tagged terms)")
+    else:
+        dom_bytes = B * (sp["merge_in"] + sp["merge_out"])
+        dom_kernel = "k_merge<2,0> (merge + reduce-by-key + filter, 40-byte batched terms)"
+    achieved = dom_bytes / sp["t_merge"] / 1e9 if sp["t_merge"] > 0 else None
     hbm, src = peaks()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -442,7 +452,7 @@ def run_ours_batch(args):
             "gpu_launches": launches * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                         "kernel": "k_merge<2,0> (merge + reduce-by-key + filter, 40-byte batched terms)",
+                         "kernel": dom_kernel, "bucket_rotations": sp["bucket_rot"],
                          "peak_source": src, "t_merge_s": sp["t_merge"], "t_rotate_s": sp["t_rotate"],
                          "t_partition_commit_s": sp["t_partition"]},
             "cpu_baseline": cpu,
