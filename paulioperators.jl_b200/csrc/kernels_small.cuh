@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_small_run(Bufs B) {
     __shared__ int s_cnt[2][3];                    // per rotation parity: outputs, sin branches, pre-filtered
     __shared__ double s_red[SM_THREADS / 32];
     __shared__ double s_expw[130], s_expxw[130];
-    __shared__ GenRec g;
+    __shared__ __align__(16) GenRec gs[2];         // this rotation's generator and the next one (prefetched)
+    static_assert(sizeof(GenRec) % 16 == 0, "generator records copy in 16-byte pieces");
+    constexpr int GQ = (int)(sizeof(GenRec) / 16);
     extern __shared__ u64 sm[];
     // term sets t = 0, 1: keys (NW words, stride C2) and coefficients
     auto tz = [&](int t) { return sm + t * (2 * NW + 1) * C2; };
@@ -120,13 +122,23 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_small_run(Bufs B) {
     if (tid < 6) (&s_cnt[0][0])[tid] = 0;
     long long rot = S->rot;
     const long long rot_end = S->rot_end;
+    // the first generator; later ones are copied in during the rotation before
+    auto fetch_gen = [&](int slot, long long q) {
+        if (tid < GQ) {
+            cp_async16(reinterpret_cast<char *>(&gs[slot]) + 16 * tid, reinterpret_cast<const char *>(B.gens + q) + 16 * tid);
+            cp_async_commit();
+        }
+    };
+    fetch_gen(0, rot);
+    if (tid < GQ) cp_async_wait_all();
     long long acap = S->acap_logical;
     long long created = 0, merge_in = 0, merge_out = 0, live_in = 0, early = 0, peak = S->peak;
     bool measure_last = false;
 
     for (int par = 0;; par ^= 1) {
-        if (tid == 0) g = B.gens[rot];
         __syncthreads();
+        const GenRec &g = gs[par];
+        if (rot + 1 < rot_end) fetch_gen(par ^ 1, rot + 1);   // the previous readers of that slot passed the barrier
         // the next rotation's counters start from zero (their last readers passed this barrier)
         if (tid < 3) s_cnt[par ^ 1][tid] = 0;
         const bool pref = n > acap;
@@ -240,6 +252,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_small_run(Bufs B) {
         n = min(total, C2);
         li ^= 1;
         ++rot;
+        if (tid < GQ) cp_async_wait_all();   // the next generator has landed (published by the next barrier)
         if (rot >= rot_end || n > C) break;
     }
     __syncthreads();
