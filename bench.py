@@ -60,10 +60,11 @@ BYTES_PER_TERM = {1: 24, 2: 40}     # B = 2*(W/8) + 8
 # dram__bytes_write.sum = 115.1 MB per launch against B(n + a + m) = 150.9 MB:
 # the gathered sin branches re-read live terms that are still in L2)
 MERGE_TRAFFIC_PER_ALG_BYTE = 115.09 / 150.88
-# DRAM traffic of k_bk_rotate<1,256,4> per algorithmic byte, from one ncu capture of
+# DRAM traffic of k_bk_rotate<1,512,4> per algorithmic byte, from one ncu capture of
 # three launches of this workload at n = 1.90e6 live terms: (dram__bytes_read.sum +
-# dram__bytes_write.sum) = 86.9 MB per launch against B(n_in + n_out) = 91.0 MB
-BUCKET_TRAFFIC_PER_ALG_BYTE = 86.91 / 91.02
+# dram__bytes_write.sum) = 60.6 MB per launch against B(n_in + n_out) = 91.0 MB (part
+# of a launch's writes is still in L2 when it ends and is written back later)
+BUCKET_TRAFFIC_PER_ALG_BYTE = 60.58 / 91.02
 
 
 def parse():
@@ -647,7 +648,8 @@ def _measure(args, wname, ws, rank, local, dev, orc):
         ps[(z, x)] = c
     obs_z, obs_x = pp.pack_keys(w.N, list(ps.keys()))
     obs_c = np.array(list(ps.values()), dtype=np.float64)
-    order = np.lexsort(tuple(obs_x[:, k] for k in range(nw - 1, -1, -1)) + tuple(obs_z[:, k] for k in range(nw - 1, -1, -1)))
+    # key order: z then x, each as an integer whose last word is the most significant
+    order = np.lexsort(tuple(obs_x[:, k] for k in range(nw)) + tuple(obs_z[:, k] for k in range(nw)))
     obs_z, obs_x, obs_c = obs_z[order], obs_x[order], obs_c[order]
     dz = torch.from_numpy(obs_z.copy()).to(dev)
     dx = torch.from_numpy(obs_x.copy()).to(dev)

@@ -317,6 +317,36 @@ int pp_get_tuning(pp_spv *h, pp_tuning *t);
  * tuning cache). */
 int pp_device_info(pp_spv *h, int32_t *sm_count, int32_t *cc_major, int32_t *cc_minor);
 
+/* Key-sharded window-1 evolution over 2^rank_bits ranks (no counterpart in the
+ * reference, whose evolve! runs in one process; spv_kernels.jl:3-5 names a
+ * multi-device engine as future work).  Rank r holds the keys P with owner(P) = r,
+ * owner being rank_bits GF(2)-linear parities of P (pp_shard_owner, host-side);
+ * the sin branch P xor M then belongs to rank r xor owner(M), so each rotation
+ * exchanges terms with one partner rank.  Per rotation r, on every rank:
+ *   pp_shard_send   packs into device buffers the local terms that anticommute
+ *                   with G_r and survive the early-merge pre-filter (pref), and
+ *                   names the partner rank (itself when nothing is to be sent);
+ *   the caller moves them to the partner (NCCL, peer copies, ...);
+ *   pp_shard_recv   takes the partner's terms (device buffers) as foreign terms;
+ *   pp_shard_rotate runs the rotation: stats5 = local {terms in, terms out, sin
+ *                   branches created, pre-filter survivors, largest bucket}.
+ * The caller sums the counts over ranks for the early-merge rule
+ * (spv_evolve.jl:356-362: pref = global n > append capacity) and, when the
+ * largest bucket of any rank passes bucket_cap / 2, calls pp_shard_regrid with
+ * one more bucket bit on every rank.  pp_shard_begin takes the call's options
+ * (window 1, a compiled truncation, no correction, no WindowCounters) and the
+ * bucket bits every rank uses; pp_shard_end returns the local set to the dense
+ * sorted layout and gives this shard's part of <ket|O|ket>. */
+int pp_shard_owner(int32_t nw, const void *z, const void *x, int64_t n, int32_t rank_bits, int32_t *owner);
+int pp_shard_begin(pp_spv *h, int32_t rank_bits, int32_t rank, const void *gz, const void *gx, const double *cosv,
+                   const double *sinv, int64_t L, const pp_evolve_opts *opts, int32_t bits, int32_t *maxcnt);
+int pp_shard_send(pp_spv *h, int64_t r, int32_t pref, void *z_out, void *x_out, double *c_out, int64_t cap,
+                  int64_t *n_out, int32_t *partner);
+int pp_shard_recv(pp_spv *h, const void *z, const void *x, const double *c, int64_t n);
+int pp_shard_rotate(pp_spv *h, int64_t r, int32_t pref, int64_t *stats5);
+int pp_shard_regrid(pp_spv *h, int32_t bits, int32_t *maxcnt);
+int pp_shard_end(pp_spv *h, double *expect_partial, double *stats_out);
+
 /* Test hooks for failure detection (no counterpart in the reference, which has no
  * device).  pp_debug_fail_alloc: the after-th next device allocation of any handle
  * fails with PP_OUT_OF_MEMORY, once (after <= 0 disarms); every growth is

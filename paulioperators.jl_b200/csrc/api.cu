@@ -143,6 +143,14 @@ struct pp_spv {
     long long bk_graph_gen = -1;
     pp_tuning tune = {BK_DEFAULT_CAP, BK_DEFAULT_ITEMS, 6, 128};  // pp_set_tuning
     struct { int occ1 = 1, occ2 = 1, occb = 1; } bk_occ[8];        // resident CTAs per SM of each variant
+    // key-sharded runs (pp_shard_*): foreign-term counts per bucket of each set,
+    // this rank, the current layout, and a device counter for packed terms
+    int *bkfcnt[2] = {nullptr, nullptr};
+    int bkfcnt_bits = -1;
+    bool shard_on = false;
+    int shard_rank_bits = 0, shard_rank = 0, shard_cur = 0, shard_bits = 0;
+    long long shard_L = 0;
+    unsigned long long *shard_cnt = nullptr;
 };
 
 // ------------------------------------------------------------------ helpers
@@ -709,7 +717,7 @@ extern "C" int pp_destroy(pp_spv *h) {
     for (int i = 0; i < 3; ++i) if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
     for (auto &kv : h->bk_graphs) cudaGraphExecDestroy(kv.second);
     void *bptrs[] = {h->bkz[0], h->bkz[1], h->bkx[0], h->bkx[1], h->bkc[0], h->bkc[1], h->bkcnt[0], h->bkcnt[1],
-                     h->bk_rows, h->bk_rec, h->bk_off, h->bk_aux};
+                     h->bk_rows, h->bk_rec, h->bk_off, h->bk_aux, h->bkfcnt[0], h->bkfcnt[1], h->shard_cnt};
     for (void *p : bptrs) if (p) cudaFree(p);
     if (h->Ph) cudaFreeHost(h->Ph);
     if (h->gens_h) cudaFreeHost(h->gens_h);
@@ -900,9 +908,7 @@ static void bk_launch(pp_spv *h, const BkVariant *v, const BkArgs &A, int k) {
 
 // Hash rows: fixed pseudo-random words (splitmix64 from a fixed seed), so the
 // bucket of a key never depends on the call.
-static int bk_rows_init(pp_spv *h) {
-    if (h->bk_rows) return PP_OK;
-    u64 rows[BK_ROWS * 4];
+static void bk_rows_host(u64 *rows) {
     unsigned long long s = 0x5EEDB0C4E7ull;
     for (int i = 0; i < BK_ROWS * 4; ++i) {
         s += 0x9E3779B97F4A7C15ull;
@@ -911,6 +917,12 @@ static int bk_rows_init(pp_spv *h) {
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         rows[i] = z ^ (z >> 31);
     }
+}
+
+static int bk_rows_init(pp_spv *h) {
+    if (h->bk_rows) return PP_OK;
+    u64 rows[BK_ROWS * 4];
+    bk_rows_host(rows);
     u64 *dr = nullptr;
     int *da = nullptr;
     TRY(dalloc(h, &dr, BK_ROWS * 4));
@@ -957,6 +969,7 @@ static BkArgs bk_args(pp_spv *h, const BkVariant *v, int bits, BkRec *rec) {
     A.S = h->S;
     A.P = h->P;
     A.gens = h->gens;
+    A.pref_forced = -1;
     if (h->batch_on) {
         A.bcos = h->bcos;
         A.bsin = h->bsin;
@@ -1065,6 +1078,8 @@ static void bk_release(pp_spv *h) {
     dfree(h, h->bk_off);
     h->bk_off = nullptr;
     h->bk_bits_cap = -1;
+    for (int q = 0; q < 2; ++q) { dfree(h, h->bkfcnt[q]); h->bkfcnt[q] = nullptr; }
+    h->bkfcnt_bits = -1;
     h->buf_gen++;
 }
 
@@ -2373,6 +2388,310 @@ extern "C" int pp_evolve_batch(pp_spv *h, const void *gz, const void *gx, int64_
         }
     }
     return r;
+}
+
+// ------------------------------------------------------------------ key-sharded runs
+// One rank of a window-1 evolution whose live set is split over 2^rank_bits ranks
+// by owner(P) (bk_owner: GF(2)-linear, so a term's sin branch P xor M is owned by
+// owner(P) xor owner(M)).  Per rotation r the caller (one process per GPU, or one
+// process driving several handles) runs, on every rank:
+//   pp_shard_send   the local terms whose sin branches the partner rank owns;
+//   (exchange them with the partner rank r xor owner(M); nothing when equal)
+//   pp_shard_recv   the partner's terms, as foreign terms of this rank's buckets;
+//   pp_shard_rotate one k_bk_rotate launch: own outputs of local terms, sin
+//                   branches of foreign terms whose partner is absent here;
+// and agrees on the global counts (early-merge rule, splits) between rotations.
+// All ranks use the same bucket count, so a bucket never holds more than cap/2
+// local plus cap/2 foreign terms.
+
+static int shard_fcnt(pp_spv *h) {
+    // foreign counts for the current bucket capacity, zeroed
+    if (h->bkfcnt_bits < h->bk_bits_cap || !h->bkfcnt[0]) {
+        int *f0 = nullptr, *f1 = nullptr;
+        TRY(dalloc(h, &f0, 1ll << h->bk_bits_cap));
+        int r = dalloc(h, &f1, 1ll << h->bk_bits_cap);
+        if (r) { dfree(h, f0); return r; }
+        dfree(h, h->bkfcnt[0]);
+        dfree(h, h->bkfcnt[1]);
+        h->bkfcnt[0] = f0;
+        h->bkfcnt[1] = f1;
+        h->bkfcnt_bits = h->bk_bits_cap;
+    }
+    CU(cudaMemsetAsync(h->bkfcnt[0], 0, sizeof(int) << h->bkfcnt_bits, h->stream));
+    CU(cudaMemsetAsync(h->bkfcnt[1], 0, sizeof(int) << h->bkfcnt_bits, h->stream));
+    return PP_OK;
+}
+
+extern "C" int pp_shard_owner(int32_t nw, const void *z, const void *x, int64_t n, int32_t rank_bits, int32_t *owner) {
+    if (nw < 1 || nw > 2 || n < 0 || rank_bits < 0 || rank_bits > 8)
+        return fail(PP_ARGUMENT_ERROR, "need nw in 1..2, n >= 0, rank_bits in 0..8");
+    if (n > 0 && (!z || !x || !owner)) return fail(PP_ARGUMENT_ERROR, "null array");
+    u64 rows[BK_ROWS * 4];
+    bk_rows_host(rows);
+    for (int64_t i = 0; i < n; ++i) {
+        u64 kz[2] = {0, 0}, kx[2] = {0, 0};
+        memcpy(kz, (const char *)z + i * nw * 8, nw * 8);
+        memcpy(kx, (const char *)x + i * nw * 8, nw * 8);
+        owner[i] = (int32_t)(nw == 1 ? bk_owner<1>(kz, kx, rows, rank_bits) : bk_owner<2>(kz, kx, rows, rank_bits));
+    }
+    return PP_OK;
+}
+
+template <int NW>
+static int shard_begin_impl(pp_spv *h, int bits, int32_t *maxcnt) {
+    TRY(ensure_dense(h));
+    TRY(bk_rows_init(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    int cur = 0;
+    const int rr = bk_reserve<NW>(h, bits, &cur, -1);
+    if (rr == BK_NOFIT) return fail(PP_OUT_OF_MEMORY, "the bucket layout of this shard does not fit in device memory");
+    if (rr) return rr;
+    int mx = 0;
+    TRY(bk_scatter<NW>(h, h->z[st.cur], h->x[st.cur], h->c[st.cur], st.n, -1, 0, 0, bits, &mx));
+    if (mx < 0) mx = h->bk_cap + 1;       // a full bucket: more buckets needed
+    TRY(shard_fcnt(h));
+    *maxcnt = mx;
+    return PP_OK;
+}
+
+extern "C" int pp_shard_begin(pp_spv *h, int32_t rank_bits, int32_t rank, const void *gz, const void *gx,
+                              const double *cosv, const double *sinv, int64_t L, const pp_evolve_opts *opts,
+                              int32_t bits, int32_t *maxcnt) {
+    if (!h || !maxcnt) return fail(PP_ARGUMENT_ERROR, "null argument");
+    if (rank_bits < 0 || rank_bits > 8 || rank < 0 || rank >= (1 << rank_bits))
+        return fail(PP_ARGUMENT_ERROR, "need rank_bits in 0..8 and 0 <= rank < 2^rank_bits");
+    if (bits < 1 || bits + rank_bits > BK_ROWS) return fail(PP_ARGUMENT_ERROR, "need 1 <= bits <= 26 - rank_bits");
+    if (L < 1 || !gz || !gx || !cosv || !sinv) return fail(PP_ARGUMENT_ERROR, "need L >= 1 generators");
+    if (h->batch_on) return fail(PP_ARGUMENT_ERROR, "a batched handle cannot be a shard");
+    pp_evolve_opts O;
+    memset(&O, 0, sizeof O);
+    O.window = 1;
+    O.chan_kind = -1;
+    if (opts) O = *opts;
+    if (O.window != 1 || O.strict_kind != 0 || O.corr_kind != 0 || O.counters)
+        return fail(PP_NOT_IMPLEMENTED, "key-sharded runs take window 1, a compiled truncation, no correction and "
+                                        "no WindowCounters");
+    DevParams *P = h->Ph;
+    compile_filter(O.strict, &P->strict);
+    compile_filter(O.local, &P->local);
+    P->local_active = filter_is_nofilter(O.local) ? 0 : 1;
+    P->corr_kind = 0;
+    load_word(O.ket, h->NW, P->ket);
+    P->chan_kind = -1;
+    if (O.chan_kind >= 0) TRY(build_channel(h, O.chan_kind, O.chan_prm, O.chan_mask, P));
+    TRY(upload_params(h));
+    TRY(ensure_gens(h, L));
+    std::vector<GenRec> G((size_t)L);
+    const size_t wb = (size_t)h->NW * 8;
+    for (long long i = 0; i < L; ++i) {
+        u64 wz[2] = {0, 0}, wx[2] = {0, 0};
+        memcpy(wz, (const char *)gz + i * wb, wb);
+        memcpy(wx, (const char *)gx + i * wb, wb);
+        bool stc = true;
+        make_gen(h, wz, wx, cosv[i], sinv[i], &G[i], &stc);
+    }
+    if (O.chan_kind >= 0) {
+        if (O.chan_every > 0) {
+            for (long long i = O.chan_every - 1; i < L; i += O.chan_every) G[i].flags |= GEN_CHANNEL;
+        } else {
+            G[L - 1].flags |= GEN_CHANNEL;
+        }
+    }
+    memcpy(h->gens_h, G.data(), L * sizeof(GenRec));
+    CU(cudaMemcpyAsync(h->gens, h->gens_h, L * sizeof(GenRec), cudaMemcpyHostToDevice, h->stream));
+    DevState st;
+    TRY(read_state(h, &st));
+    st.rot = 0;
+    st.rot_end = L;
+    st.created = st.merge_in = st.merge_out = st.early = 0;
+    st.npref = st.live_in = st.peak = 0;
+    st.measure_valid = 0;
+    st.err = 0;
+    TRY(write_state(h, &st));
+    if (L + 1 > h->bk_rec_cap) {
+        TRY(dalloc(h, &h->bk_rec, L + 1));
+        h->bk_rec_cap = L + 1;
+    }
+    {
+        BkRec r0;
+        memset(&r0, 0, sizeof r0);
+        r0.n_in = st.n;
+        r0.n_out = (unsigned long long)st.n;
+        r0.acap = 1ll << 62;
+        CU(cudaMemcpyAsync(h->bk_rec, &r0, sizeof r0, cudaMemcpyHostToDevice, h->stream));
+        CU(cudaMemsetAsync(h->bk_rec + 1, 0, L * sizeof(BkRec), h->stream));
+    }
+    if (!h->shard_cnt) TRY(dalloc(h, &h->shard_cnt, 1));
+    TRY(h->NW == 1 ? shard_begin_impl<1>(h, bits, maxcnt) : shard_begin_impl<2>(h, bits, maxcnt));
+    h->shard_on = true;
+    h->shard_rank_bits = rank_bits;
+    h->shard_rank = rank;
+    h->shard_cur = 0;
+    h->shard_bits = bits;
+    h->shard_L = L;
+    return PP_OK;
+}
+
+static int shard_partner(pp_spv *h, int64_t r, int32_t *partner) {
+    if (!h->shard_on) return fail(PP_ARGUMENT_ERROR, "no key-sharded run in progress (pp_shard_begin)");
+    if (r < 0 || r >= h->shard_L) return fail(PP_ARGUMENT_ERROR, "rotation index out of range");
+    u64 rows[BK_ROWS * 4];
+    bk_rows_host(rows);
+    const GenRec &g = h->gens_h[r];
+    const unsigned o = h->NW == 1 ? bk_owner<1>(g.gz, g.gx, rows, h->shard_rank_bits)
+                                  : bk_owner<2>(g.gz, g.gx, rows, h->shard_rank_bits);
+    *partner = h->shard_rank ^ (int32_t)o;
+    return PP_OK;
+}
+
+extern "C" int pp_shard_send(pp_spv *h, int64_t r, int32_t pref, void *zout, void *xout, double *cout, int64_t cap,
+                             int64_t *n_out, int32_t *partner) {
+    if (!h || !n_out || !partner) return fail(PP_ARGUMENT_ERROR, "null argument");
+    TRY(shard_partner(h, r, partner));
+    *n_out = 0;
+    if (*partner == h->shard_rank) return PP_OK;
+    if (cap > 0 && (!zout || !xout || !cout)) return fail(PP_ARGUMENT_ERROR, "null output buffer");
+    cudaStream_t s = h->stream;
+    CU(cudaMemsetAsync(h->shard_cnt, 0, sizeof(unsigned long long), s));
+    const int cur = h->shard_cur, bits = h->shard_bits, cap_b = h->bk_cap;
+    const long long slots = (long long)cap_b << bits;
+    const int grid = (int)std::max(1ll, std::min((slots + 255) / 256, (long long)h->nsm * 16));
+    if (h->NW == 1)
+        k_bk_send<1><<<grid, 256, 0, s>>>(h->bkz[cur], h->bkx[cur], h->bkc[cur], h->bkcnt[cur], bits, cap_b,
+                                          h->gens + r, pref ? 1 : 0, h->P, (u64 *)zout, (u64 *)xout, cout, cap,
+                                          h->shard_cnt, h->S);
+    else
+        k_bk_send<2><<<grid, 256, 0, s>>>(h->bkz[cur], h->bkx[cur], h->bkc[cur], h->bkcnt[cur], bits, cap_b,
+                                          h->gens + r, pref ? 1 : 0, h->P, (u64 *)zout, (u64 *)xout, cout, cap,
+                                          h->shard_cnt, h->S);
+    unsigned long long n = 0;
+    CU(cudaMemcpyAsync(&n, h->shard_cnt, sizeof n, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    if (st.err & ERR_OVERFLOW) {
+        st.err &= ~ERR_OVERFLOW;
+        TRY(write_state(h, &st));
+        return fail(PP_OUT_OF_MEMORY, "pp_shard_send: " + std::to_string(n) + " terms to send, buffer holds " +
+                                          std::to_string(cap));
+    }
+    TRY(check_err(h, st));
+    *n_out = (int64_t)n;
+    return PP_OK;
+}
+
+extern "C" int pp_shard_recv(pp_spv *h, const void *z, const void *x, const double *c, int64_t n) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    if (!h->shard_on) return fail(PP_ARGUMENT_ERROR, "no key-sharded run in progress (pp_shard_begin)");
+    if (n < 0 || (n > 0 && (!z || !x || !c))) return fail(PP_ARGUMENT_ERROR, "need n >= 0 received terms");
+    if (n == 0) return PP_OK;
+    cudaStream_t s = h->stream;
+    const int cur = h->shard_cur, bits = h->shard_bits;
+    const int grid = (int)std::max(1ll, std::min((long long)(n + 255) / 256, (long long)h->nsm * 16));
+    if (h->NW == 1)
+        k_bk_absorb<1><<<grid, 256, 0, s>>>((const u64 *)z, (const u64 *)x, c, n, h->bkz[cur], h->bkx[cur], h->bkc[cur],
+                                            h->bkcnt[cur], h->bkfcnt[cur], bits, h->bk_cap, h->bk_rows, h->S);
+    else
+        k_bk_absorb<2><<<grid, 256, 0, s>>>((const u64 *)z, (const u64 *)x, c, n, h->bkz[cur], h->bkx[cur], h->bkc[cur],
+                                            h->bkcnt[cur], h->bkfcnt[cur], bits, h->bk_cap, h->bk_rows, h->S);
+    TRY(sync_check(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    if (st.err & ERR_OVERFLOW) return fail(PP_OUT_OF_MEMORY, "pp_shard_recv: a bucket would exceed its capacity");
+    return check_err(h, st);
+}
+
+template <int NW>
+static int shard_rotate_impl(pp_spv *h, int64_t r, int pref, int remote, int64_t *out) {
+    const BkVariant *var = bk_variant(h->tune.bucket_cap, h->tune.items_per_thread);
+    if (!var || var->cap != h->bk_cap) return fail(PP_ERROR_EXCEPTION, "internal error: bucket variant changed");
+    cudaStream_t s = h->stream;
+    BkArgs A = bk_args(h, var, h->shard_bits, h->bk_rec);
+    A.fcnt[0] = h->bkfcnt[0];
+    A.fcnt[1] = h->bkfcnt[1];
+    A.remote = remote;
+    A.pref_forced = pref ? 1 : 0;
+    k_bk_begin<<<1, 1, 0, s>>>(h->S, r, h->shard_cur, 1);
+    bk_launch<NW>(h, var, A, 0);
+    BkRec o;
+    CU(cudaMemcpyAsync(&o, h->bk_rec + r + 1, sizeof o, cudaMemcpyDeviceToHost, s));
+    TRY(sync_check(h));
+    DevState st;
+    TRY(read_state(h, &st));
+    if (st.err & ERR_OVERFLOW) return fail(PP_OUT_OF_MEMORY, "pp_shard_rotate: a bucket would exceed its capacity");
+    TRY(check_err(h, st));
+    h->shard_cur ^= 1;
+    st.live_in += o.n_in;
+    st.created += (long long)o.created;
+    st.merge_in += o.n_in + (long long)o.created;
+    st.merge_out += (long long)o.n_out;
+    if ((long long)o.n_out > st.peak) st.peak = (long long)o.n_out;
+    if (pref) st.early += 1;
+    st.rot = r + 1;
+    TRY(write_state(h, &st));
+    out[0] = o.n_in;
+    out[1] = (int64_t)o.n_out;
+    out[2] = (int64_t)o.created;
+    out[3] = (int64_t)o.np;
+    out[4] = o.maxcnt;
+    return PP_OK;
+}
+
+extern "C" int pp_shard_rotate(pp_spv *h, int64_t r, int32_t pref, int64_t *stats5) {
+    if (!h || !stats5) return fail(PP_ARGUMENT_ERROR, "null argument");
+    int32_t partner = 0;
+    TRY(shard_partner(h, r, &partner));
+    const int remote = partner != h->shard_rank ? 1 : 0;
+    return h->NW == 1 ? shard_rotate_impl<1>(h, r, pref, remote, stats5) : shard_rotate_impl<2>(h, r, pref, remote, stats5);
+}
+
+template <int NW>
+static int shard_regrid_impl(pp_spv *h, int bits, int32_t *maxcnt) {
+    int cur = h->shard_cur;
+    const int rr = bk_reserve<NW>(h, bits, &cur, h->shard_bits);
+    if (rr == BK_NOFIT) return fail(PP_OUT_OF_MEMORY, "the bucket layout of this shard does not fit in device memory");
+    if (rr) return rr;
+    int mx = 0;
+    TRY(bk_scatter<NW>(h, h->bkz[cur], h->bkx[cur], h->bkc[cur], 0, cur, h->shard_bits, cur ^ 1, bits, &mx));
+    if (mx < 0) mx = h->bk_cap + 1;
+    h->shard_cur = cur ^ 1;
+    h->shard_bits = bits;
+    TRY(shard_fcnt(h));
+    *maxcnt = mx;
+    return PP_OK;
+}
+
+extern "C" int pp_shard_regrid(pp_spv *h, int32_t bits, int32_t *maxcnt) {
+    if (!h || !maxcnt) return fail(PP_ARGUMENT_ERROR, "null argument");
+    if (!h->shard_on) return fail(PP_ARGUMENT_ERROR, "no key-sharded run in progress (pp_shard_begin)");
+    if (bits < 1 || bits + h->shard_rank_bits > BK_ROWS) return fail(PP_ARGUMENT_ERROR, "need 1 <= bits <= 26 - rank_bits");
+    return h->NW == 1 ? shard_regrid_impl<1>(h, bits, maxcnt) : shard_regrid_impl<2>(h, bits, maxcnt);
+}
+
+extern "C" int pp_shard_end(pp_spv *h, double *expect_partial, double *stats_out) {
+    if (!h) return fail(PP_ARGUMENT_ERROR, "null handle");
+    if (!h->shard_on) return fail(PP_ARGUMENT_ERROR, "no key-sharded run in progress (pp_shard_begin)");
+    h->shard_on = false;
+    TRY(h->NW == 1 ? bk_to_dense<1>(h, h->shard_cur, h->shard_bits) : bk_to_dense<2>(h, h->shard_cur, h->shard_bits));
+    double ev = 0.0;
+    TRY(expect_dev(h, h->Ph->ket, &ev));
+    DevState st;
+    TRY(read_state(h, &st));
+    st.expect_val = ev;
+    st.measure_valid = 1;
+    TRY(write_state(h, &st));
+    if (expect_partial) *expect_partial = ev;
+    if (stats_out) {
+        for (int i = 0; i < PP_STATS_LEN; ++i) stats_out[i] = 0.0;
+        stats_out[PP_STAT_TERMS_IN] = (double)st.live_in;
+        stats_out[PP_STAT_CREATED] = (double)st.created;
+        stats_out[PP_STAT_MERGE_IN] = (double)st.merge_in;
+        stats_out[PP_STAT_MERGE_OUT] = (double)st.merge_out;
+        stats_out[PP_STAT_PEAK] = (double)st.peak;
+        stats_out[PP_STAT_EARLY] = (double)st.early;
+    }
+    return PP_OK;
 }
 
 // ------------------------------------------------------------------ learned truncation

@@ -117,6 +117,15 @@ constexpr int G_ITEMS = 8;
 constexpr int G_TILE = G_THREADS * G_ITEMS;   // general rotate tile
 constexpr int SPIN_LIMIT = 1 << 22;           // bounded look-back waits
 
+// Population count usable in host and device code.
+__host__ __device__ __forceinline__ int popc64(u64 v) {
+#ifdef __CUDA_ARCH__
+    return __popcll(v);
+#else
+    return __builtin_popcountll(v);
+#endif
+}
+
 // mbarrier in shared memory (addresses are shared-window addresses).
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 

@@ -77,6 +77,13 @@ struct BkArgs {
     const long long *bend;
     long long ninst;
     int ncol;
+    // key-sharded runs: per bucket, foreign terms (received from the partner rank)
+    // follow the local ones; remote: the sin branches of local terms belong to the
+    // partner rank; pref_forced: the early-merge decision from the global counts
+    // (-1: from the rotation record, as on one rank)
+    int *fcnt[2];
+    int remote;
+    int pref_forced;
 };
 
 // Bucket of a key: the low `bits` bits of the GF(2)-linear hash.
@@ -246,13 +253,14 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     const int cur = (S->bk_cur0 + k) & 1;
     __shared__ GenRec g;
     __shared__ unsigned s_delta;
-    __shared__ int s_b[2][NBK], s_n[2][NBK], s_off[2][NBK + 1], s_j1[2];
+    __shared__ int s_b[2][NBK], s_n[2][NBK], s_nl[2][NBK], s_off[2][NBK + 1], s_j1[2];
     __shared__ int s_out[NBK], s_mx, s_bad;
     __shared__ int s_red[3][T / 32];
     extern __shared__ __align__(128) u64 bsm[];
     // staging area a: keys (NW words each, z then x), coefficients; then the key
-    // index and, per area, each staged term's local bucket (bit 7: dropped by the
-    // early merge)
+    // index and, per area, a byte per staged slot: its local bucket in bits 0-5,
+    // bit 6 for a foreign term (key-sharded runs), bit 7 when the slot holds no
+    // term (a run's padding slot) or one the early merge drops
     constexpr int AREA = (2 * NW + 1) * SMI;       // u64 words of one staging area
     auto skz = [&](int a) { return bsm + a * AREA; };
     auto skx = [&](int a) { return bsm + a * AREA + NW * SMI; };
@@ -287,7 +295,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     const long long n_r = (long long)prev.n_out;
     long long acap = prev.acap;
     if (prev.pref && (long long)prev.np > acap) acap = max(2 * acap, (long long)prev.np);
-    const bool pref = n_r > acap;
+    const bool pref = A.pref_forced >= 0 ? A.pref_forced != 0 : n_r > acap;
     if (blockIdx.x == 0 && tid == 0) {
         BkRec &me = A.rec[r + 1];
         me.n_in = n_r;
@@ -307,6 +315,9 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     // (selected, not indexed: a runtime index into the parameter struct would copy it to the stack)
     const int *CNT = cur ? A.cnt[1] : A.cnt[0];
     int *OCNT = cur ? A.cnt[0] : A.cnt[1];
+    const int *FCNT = A.fcnt[0] ? (cur ? A.fcnt[1] : A.fcnt[0]) : nullptr;
+    int *OFCNT = A.fcnt[0] ? (cur ? A.fcnt[0] : A.fcnt[1]) : nullptr;
+    const bool remote = A.remote != 0;
     const u64 *Z = cur ? A.z[1] : A.z[0], *X = cur ? A.x[1] : A.x[0];
     const double *C = cur ? A.c[1] : A.c[0];
     u64 *OZ = cur ? A.z[0] : A.z[1], *OX = cur ? A.x[0] : A.x[1];
@@ -321,22 +332,24 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     // pair buckets and counts of group gi into area a (threads < G); -1 group: none
     auto load_info = [&](int a, long long gi) {
         if (tid < G) {
-            int b0 = 0, b1 = 0, n0 = 0, n1 = 0;
+            int b0 = 0, b1 = 0, n0 = 0, n1 = 0, f0 = 0, f1 = 0;
             if (gi >= 0) {
                 bk_pair(delta, gi * G + tid, &b0, &b1);
                 if (b0 < 0 || b1 < 0 || b0 >= nb || b1 >= nb) { flag_bounds(S, 3, b0); s_bad = 1; b0 = b1 = 0; }
                 else {
                     n0 = CNT[b0];
                     n1 = CNT[b1];
-                    if (n0 < 0 || n1 < 0 || n0 > CAP || n1 > CAP) {
+                    if (FCNT) { f0 = FCNT[b0]; f1 = FCNT[b1]; }
+                    if (n0 < 0 || n1 < 0 || f0 < 0 || f1 < 0 || n0 + f0 > CAP || n1 + f1 > CAP) {
                         flag_bounds(S, 4, ((long long)n0 << 20) | (n1 & 0xfffff));
                         s_bad = 1;
-                        n0 = n1 = 0;
+                        n0 = n1 = f0 = f1 = 0;
                     }
                 }
             }
             s_b[a][2 * tid] = b0; s_b[a][2 * tid + 1] = b1;
-            s_n[a][2 * tid] = n0; s_n[a][2 * tid + 1] = n1;
+            s_n[a][2 * tid] = n0 + f0; s_n[a][2 * tid + 1] = n1 + f1;
+            s_nl[a][2 * tid] = n0; s_nl[a][2 * tid + 1] = n1;
         }
     };
     // first sub-group [j0, j1) of pairs from j0 that fits the staging area, and its
@@ -385,6 +398,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         for (int lb = warp; lb < nloc; lb += T / 32) {
             const int bq = s_b[a][2 * j0 + lb];
             const int o0 = s_off[a][lb], len = s_off[a][lb + 1] - o0, cnt = s_n[a][2 * j0 + lb];
+            const int loc = s_nl[a][2 * j0 + lb];     // local terms first, then foreign ones
             if (bq < 0 || bq >= nb || len < 0 || len > CAP || (o0 & 1) || (len & 1)) {
                 if (lane == 0) flag_bounds(S, 6, ((long long)bq << 20) | (len & 0xfffff));
                 for (int t = lane; t < len; t += 32) sbk[o0 + t] = (unsigned char)(0x80 | lb);
@@ -401,8 +415,8 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     cp_async16(skx(a) + NW * i + 2 * w, X + NW * p + 2 * w);
                 }
                 cp_async16(sc(a) + i, C + p);
-                sbk[i] = (unsigned char)(t < cnt ? lb : (0x80 | lb));
-                sbk[i + 1] = (unsigned char)(t + 1 < cnt ? lb : (0x80 | lb));
+                sbk[i] = (unsigned char)(t < loc ? lb : t < cnt ? (0x40 | lb) : (0x80 | lb));
+                sbk[i + 1] = (unsigned char)(t + 1 < loc ? lb : t + 1 < cnt ? (0x40 | lb) : (0x80 | lb));
             }
         }
         cp_async_commit();
@@ -433,7 +447,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         for (int i = tid; i < ntot; i += T) {
             if (sbk[i] & 0x80) continue;     // a run's padding slot
             const Key<NW> kk = skey(a, i);
-            if (pref && drop_q<NW>(fs, P.strict, kk, fabs(sc(a)[i]))) {
+            if (pref && !(sbk[i] & 0x40) && drop_q<NW>(fs, P.strict, kk, fabs(sc(a)[i]))) {
                 sbk[i] |= 0x80;
                 continue;
             }
@@ -461,8 +475,9 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             // local bucket (0x7f past the staged terms keeps buckets nondecreasing
             // across the warp) and early-merge drop flag
             const int tag = i < ntot ? sbk[i] : 0x7f;
-            int lb = tag & 0x7f;
+            int lb = tag & 0x3f;
             const bool in = i < ntot && tag < 0x80;
+            const bool fgn = (tag & 0x40) != 0;      // a foreign term: its sin branch only
             if (i < ntot && lb >= 2 * (j1 - j0)) {
                 flag_bounds(S, 7, lb);
                 lb = 0;
@@ -470,7 +485,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             bool own = false, nw_ = false;
             double oval = 0.0, nval = 0.0;
             if (in) {
-                ++alive;
+                alive += fgn ? 0 : 1;
                 const Key<NW> kk = skey(a, i);
                 const double c = sc(a)[i];
                 double v = c;
@@ -495,7 +510,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     v = __dmul_rn(c, cvt);
                     const double s = __dmul_rn(sg * svt, c);     // (k - 2) * sin(theta) * c, spv_kernels.jl:163
                     const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
-                    cre += s_ok ? 1 : 0;
+                    cre += (s_ok && !fgn) ? 1 : 0;
                     const int j = find(qk);
                     if (j >= ntot) flag_bounds(S, 8, j);
                     if (j >= 0 && j < ntot) {
@@ -505,12 +520,15 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                         // (mod 4) in _rotate_range!'s k (spv_kernels.jl:162-163), and k is odd
                         const double t = __dmul_rn(-(sg * svt), sc(a)[j]);
                         if (!(local_on && should_drop<NW>(P.local, kk, fabs(t)))) v = __dadd_rn(v, t);
-                    } else if (s_ok && !drop_q<NW>(fs, P.strict, qk, fabs(s))) {
+                    } else if (s_ok && (fgn || !remote) && !drop_q<NW>(fs, P.strict, qk, fabs(s))) {
+                        // (a local term's sin branch belongs to the partner rank when remote)
                         nval = do_chan ? __dmul_rn(s, channel_factor<NW>(P, qk)) : s;
                         nw_ = true;
                     }
                 }
-                if (!act) {
+                if (fgn) {
+                    // a foreign term's own key belongs to the partner rank
+                } else if (!act) {
                     oval = v;                                    // an ended instance is kept as it is
                     own = true;
                 } else if (!drop_q<NW>(fs, P.strict, kk, fabs(v))) {
@@ -567,10 +585,14 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
         const int a = it & 1;
         const long long gnext = gi + gridDim.x, gafter = gi + 2 * (long long)gridDim.x;
         // the group after next: its pair counts load while this group is processed
-        int pb0 = 0, pb1 = 0, pn0 = 0, pn1 = 0;
+        int pb0 = 0, pb1 = 0, pn0 = 0, pn1 = 0, pf0 = 0, pf1 = 0;
         if (tid < G && gafter < ngroups) {
             bk_pair(delta, gafter * G + tid, &pb0, &pb1);
-            if (pb0 < nb && pb1 < nb) { pn0 = CNT[pb0]; pn1 = CNT[pb1]; }
+            if (pb0 < nb && pb1 < nb) {
+                pn0 = CNT[pb0];
+                pn1 = CNT[pb1];
+                if (FCNT) { pf0 = FCNT[pb0]; pf1 = FCNT[pb1]; }
+            }
         }
         staged(a);
         __syncthreads();
@@ -594,20 +616,23 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             if (lane < 2 * G) {
                 const int m = s_out[lane];
                 OCNT[s_b[a][lane]] = min(m, CAP);
+                if (OFCNT) OFCNT[s_b[a][lane]] = 0;
                 atomicMax(&s_mx, m);
                 s_out[lane] = 0;
             }
             __syncwarp();
             if (lane < G) {
                 if (gafter < ngroups) {
-                    if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pn0 > CAP || pn1 > CAP) {
+                    if (pb0 >= nb || pb1 >= nb || pn0 < 0 || pn1 < 0 || pf0 < 0 || pf1 < 0 || pn0 + pf0 > CAP ||
+                        pn1 + pf1 > CAP) {
                         flag_bounds(S, 10, ((long long)pn0 << 20) | (pn1 & 0xfffff));
                         s_bad = 1;
-                        pb0 = pb1 = pn0 = pn1 = 0;
+                        pb0 = pb1 = pn0 = pn1 = pf0 = pf1 = 0;
                     }
                 }
                 s_b[a][2 * lane] = pb0; s_b[a][2 * lane + 1] = pb1;
-                s_n[a][2 * lane] = pn0; s_n[a][2 * lane + 1] = pn1;
+                s_n[a][2 * lane] = pn0 + pf0; s_n[a][2 * lane + 1] = pn1 + pf1;
+                s_nl[a][2 * lane] = pn0; s_nl[a][2 * lane + 1] = pn1;
             }
             __syncwarp();
             plan(a, 0);
@@ -711,6 +736,80 @@ __global__ void k_bk_gather(const u64 *SZ, const u64 *SX, const double *SC, cons
             store_key<NW>(DZ, DX, o + j, load_key<NW>(SZ, SX, s));
             DC[o + j] = SC[s];
         }
+    }
+}
+
+// Owner rank of a key in a key-sharded run over 2^rank_bits ranks: bit k is the
+// parity of P & R_(BK_ROWS - 1 - k), rows the bucket hash of a layout with at most
+// BK_ROWS - rank_bits row bits never uses.  Linear like the bucket hash, so the
+// sin branch P xor M of a term owned by r is owned by r xor owner(M).
+template <int NW>
+__host__ __device__ __forceinline__ unsigned bk_owner(const u64 *kz, const u64 *kx, const u64 *rows, int rank_bits) {
+    unsigned o = 0;
+    for (int k = 0; k < rank_bits; ++k) {
+        const u64 *R = rows + 4 * (BK_ROWS - 1 - k);
+        int p = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) p += popc64(kz[w] & R[w]) + popc64(kx[w] & R[2 + w]);
+        o |= (unsigned)(p & 1) << k;
+    }
+    return o;
+}
+
+// Key-sharded runs: the local terms of bucket set (Z, X, C, CNT) that anticommute
+// with the generator and survive the early-merge pre-filter (when pref) -- the
+// terms whose sin branches belong to the partner rank -- packed into (OZ, OX, OC)
+// in any order; their number in *nout.  More than cap of them: ERR_OVERFLOW.
+template <int NW>
+__global__ void k_bk_send(const u64 *Z, const u64 *X, const double *C, const int *CNT, int bits, int cap,
+                          const GenRec *gen, int pref, const DevParams *P, u64 *OZ, u64 *OX, double *OC, long long ocap,
+                          unsigned long long *nout, DevState *S) {
+    const long long slots = (long long)cap << bits;
+    const FQuick fs = fquick(P->strict);
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < slots; base += (long long)gridDim.x * blockDim.x) {
+        const long long i = base + threadIdx.x;
+        bool send = false;
+        Key<NW> kk;
+        if (i < slots && (int)(i % cap) < CNT[i / cap]) {
+            kk = load_key<NW>(Z, X, i);
+            send = anticommutes<NW>(kk, *gen) && !(pref && drop_q<NW>(fs, P->strict, kk, fabs(C[i])));
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, send);
+        if (!m) continue;
+        const int leader = __ffs(m) - 1;
+        unsigned long long b0 = 0;
+        if (lane == leader) b0 = atomicAdd(nout, (unsigned long long)__popc(m));
+        b0 = __shfl_sync(0xffffffffu, b0, leader);
+        if (send) {
+            const long long o = (long long)b0 + __popc(m & ((1u << lane) - 1u));
+            if (o < ocap) {
+                store_key<NW>(OZ, OX, o, kk);
+                OC[o] = C[i];
+            } else {
+                atomicOr(&S->err, ERR_OVERFLOW);
+            }
+        }
+    }
+}
+
+// Key-sharded runs: n received terms appended to their buckets of the set
+// (Z, X, C) as foreign terms, after the CNT[b] local ones (FCNT[b] counts them).
+// A bucket that would exceed cap: ERR_OVERFLOW, the term is not written.
+template <int NW>
+__global__ void k_bk_absorb(const u64 *RZ, const u64 *RX, const double *RC, long long n, u64 *Z, u64 *X, double *C,
+                            const int *CNT, int *FCNT, int bits, int cap, const u64 *rows, DevState *S) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const Key<NW> kk = load_key<NW>(RZ, RX, i);
+        const unsigned b = bk_hash<NW>(kk.z, kk.x, rows, bits);
+        const int pos = CNT[b] + atomicAdd(&FCNT[b], 1);
+        if (pos >= cap) {
+            atomicOr(&S->err, ERR_OVERFLOW);
+            continue;
+        }
+        const long long o = (long long)b * cap + pos;
+        store_key<NW>(Z, X, o, kk);
+        C[o] = RC[i];
     }
 }
 

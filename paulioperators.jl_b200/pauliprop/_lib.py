@@ -134,6 +134,15 @@ SIGNATURES = {
     "pp_debug_fail_alloc": (c_int32, [c_int64]),
     "pp_debug_lookback_timeout": (c_int32, [c_int64]),
     "pp_debug_bucket_limit": (c_int32, [c_int64]),
+    "pp_shard_owner": (c_int32, [c_int32, c_void_p, c_void_p, c_int64, c_int32, c_void_p]),
+    "pp_shard_begin": (c_int32, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                 POINTER(PPEvolveOpts), c_int32, c_void_p]),
+    "pp_shard_send": (c_int32, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p, c_int64, c_void_p,
+                                c_void_p]),
+    "pp_shard_recv": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64]),
+    "pp_shard_rotate": (c_int32, [c_void_p, c_int64, c_int32, c_void_p]),
+    "pp_shard_regrid": (c_int32, [c_void_p, c_int32, c_void_p]),
+    "pp_shard_end": (c_int32, [c_void_p, c_void_p, c_void_p]),
 }
 
 
