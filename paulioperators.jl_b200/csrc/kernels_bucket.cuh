@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                 }
             }
             const int tb = ob ^ flip;                        // the partner bucket of the pair
-            const int pn = bk_claim(s_out, tb, nw_, seg, lane);
+            const int pn = __any_sync(0xffffffffu, nw_) ? bk_claim(s_out, tb, nw_, seg, lane) : -1;   // new terms are rare
             if (nw_) {
                 if (pn < CAP) {
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
