@@ -4,8 +4,8 @@ The launch configuration of k_bk_rotate -- bucket capacity (the CTA's tile of
 terms), items per thread, the bucketing load divisor and the rotations launched
 between host checks -- changes how fast a sequence runs, never what it computes
 (every variant is checked bit for bit against the oracle in the GPU tests).
-`tune()` times each candidate on the device on a representative sequence per
-word count and writes the fastest to a JSON cache keyed by the device's SM count
+`tune()` times each candidate on the device (CUDA events on the vector's
+stream) on a representative sequence per word count and writes the fastest to a JSON cache keyed by the device's SM count
 and compute capability; `apply_cached(v)` gives a new vector the cached setting.
 
 Cache file: paulioperators.jl_b200/tuning/sm<count>_cc<major><minor>.json
@@ -20,7 +20,6 @@ import ctypes
 import json
 import os
 import sys
-import time
 
 from . import _lib
 from .circuits import lattice64
@@ -96,15 +95,22 @@ def _time_one(nw, t, reps):
     gens = [PauliBasis(N, p.z, p.x) for p in w.layer] * w.layers
     angs = list(w.angles) * w.layers
     strat = CompositeTruncation(CoeffTruncation(w.thresh), WeightTruncation(w.wmax))
+    import torch
     best = None
     for _ in range(reps + 1):     # the first run warms up (allocations, graphs)
         v = spv.SparsePauliVector.from_paulisum(ps)
         set_tuning(v, t)
         st = {}
-        t0 = time.perf_counter()
+        # device time on the vector's stream (the host time of a call would add
+        # its own overhead, comparable to the differences between candidates)
+        stream = torch.cuda.ExternalStream(v.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         spv.evolve_(v, gens, angs, truncation=strat, channel=(w.channel[0], w.channel[1], None),
                     channel_every=len(w.layer), stats=st)
-        dt = time.perf_counter() - t0
+        e1.record(stream)
+        e1.synchronize()
+        dt = e0.elapsed_time(e1) * 1e-3
         rate = st["terms_in"] / dt
         best = rate if best is None or rate > best else best
         v.close()
