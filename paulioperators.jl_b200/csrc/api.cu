@@ -220,9 +220,10 @@ static int read_state(pp_spv *h, DevState *st) {
     CU(cudaStreamSynchronize(h->stream));
     return PP_OK;
 }
+// (a copy from pageable memory: the host copy may be reused on return, and the
+// stream orders the copy before every later launch, so no synchronisation)
 static int write_state(pp_spv *h, const DevState *st) {
     CU(cudaMemcpyAsync(h->S, st, sizeof(DevState), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
     return PP_OK;
 }
 
@@ -1363,7 +1364,7 @@ static int run_bucket(pp_spv *h, long long start, long long L, pp_counters *ctr,
 // correction or batched instances, and no per-rotation timing), one launch of it
 // runs the rotations instead.
 template <int NW>
-static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof) {
+static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr, RunProf *prof, long long n_known = -1) {
     long long done = start;
     const bool per_rot = ctr && (ctr->t_rotate || ctr->t_merge);   // per-rotation times asked for
     const bool timed = prof->on || per_rot;
@@ -1372,10 +1373,15 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
     const bool small_ok = !per_rot && !h->batch_on && !h->Ph->local_active && h->Ph->corr_kind == 0;
     bool use_bk = bk_enabled() && h->Ph->corr_kind == 0;
     long long ncur = small_cap<NW>() + 1;   // live terms at the chunk's start (read when small_ok)
+    bool dense = false;                      // the last state read showed a dense live set
     if (small_ok) {
-        DevState st;
-        TRY(read_state(h, &st));
-        ncur = st.n;
+        if (n_known >= 0) {
+            ncur = n_known;
+        } else {
+            DevState st;
+            TRY(read_state(h, &st));
+            ncur = st.n;
+        }
     }
     while (done < L) {
         if (small_ok && ncur <= small_cap<NW>()) {
@@ -1388,6 +1394,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
             if (st.err) { ensure_dense(h); return check_err(h, st); }
             table = false;
             ncur = st.n;
+            dense = st.seg_dense != 0;
             if (st.rot == done) ncur = small_cap<NW>() + 1;   // no progress: leave it to the multi-kernel path
             done = st.rot;
             continue;
@@ -1407,6 +1414,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
             ncur = small_ok ? st.n : small_cap<NW>() + 1;
             continue;
         }
+        dense = false;                       // the merge kernels leave a segment table
         Bufs B = make_bufs(h);
         const long long end = std::min(L, done + CHUNK_ROT);
         cudaStream_t s = h->stream;
@@ -1490,7 +1498,7 @@ static int run_struct(pp_spv *h, long long start, long long L, pp_counters *ctr,
             table = false;
         }
     }
-    return ensure_dense(h);
+    return dense ? PP_OK : ensure_dense(h);
 }
 
 // General path boundary: sort pending appends, merge (MODE 1).
@@ -1959,8 +1967,8 @@ static int evolve_impl(pp_spv *h, const void *gz, const void *gx, const double *
             h->rec_cap = L;
         }
         if (want_rec != h->rec_on) { h->rec_on = want_rec; h->buf_gen++; }
-        if (h->NW == 1) TRY(run_struct<1>(h, 0, L, ctr, &prof));
-        else TRY(run_struct<2>(h, 0, L, ctr, &prof));
+        if (h->NW == 1) TRY(run_struct<1>(h, 0, L, ctr, &prof, st.n));
+        else TRY(run_struct<2>(h, 0, L, ctr, &prof, st.n));
         if (want_rec) {
             std::vector<long long> rec((size_t)(4 * L));
             CU(cudaMemcpy(rec.data(), h->rec, 4 * L * sizeof(long long), cudaMemcpyDeviceToHost));

@@ -191,6 +191,10 @@ def PauliSum_from(v):
 def _gen_words(N, generators):
     nw = nwords(N)
     L = len(generators)
+    if nw == 1:
+        gz = np.fromiter((g.z if type(g) is PauliBasis else int(g[0]) for g in generators), np.uint64, L)
+        gx = np.fromiter((g.x if type(g) is PauliBasis else int(g[1]) for g in generators), np.uint64, L)
+        return gz.reshape(L, 1), gx.reshape(L, 1)
     m = (1 << 64) - 1
     zs = [g.z if isinstance(g, PauliBasis) else int(g[0]) for g in generators]
     xs = [g.x if isinstance(g, PauliBasis) else int(g[1]) for g in generators]
@@ -290,8 +294,9 @@ def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=Non
     opts.profile = 1 if profile else 0
     gz, gx = _gen_words(v.N, generators)
     ang = np.asarray(angles, dtype=np.float64)
-    cosv = np.array([math.cos(a) for a in ang.tolist()], dtype=np.float64)
-    sinv = np.array([math.sin(a) for a in ang.tolist()], dtype=np.float64)
+    al = ang.tolist()
+    cosv = np.fromiter(map(math.cos, al), np.float64, len(al))     # libm, as the reference's host
+    sinv = np.fromiter(map(math.sin, al), np.float64, len(al))
     check(lib.pp_evolve(v._h, _ptr(gz), _ptr(gx), _ptr(cosv), _ptr(sinv), len(ang), byref(opts)))
     if isinstance(correction, (EnergyCorrection, EnergyVarianceCorrection)):
         correction.accumulated_energy = ce.value
