@@ -699,6 +699,12 @@ def _measure(args, wname, ws, rank, local, dev, orc):
     hz = torch.from_numpy(obs_z.copy()).pin_memory()
     hx = torch.from_numpy(obs_x.copy()).pin_memory()
     hc = torch.from_numpy(obs_c.copy()).pin_memory()
+    # pinned host buffers for the result (a caller reading tens of MB per step
+    # would allocate them once), sized for this step's final set
+    fcap = max(1, len(g))
+    pz = torch.empty((fcap, nw), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    px = torch.empty((fcap, nw), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    pc = torch.empty(fcap, dtype=torch.float64).pin_memory().numpy()
     h2d = d2h = 0
     te = []
     final = None
@@ -707,15 +713,18 @@ def _measure(args, wname, ws, rank, local, dev, orc):
             torch.distributed.barrier()
         t0 = time.perf_counter()
         pp.spv.check(pp.spv.lib.pp_upload(g._h, hz.data_ptr(), hx.data_ptr(), hc.data_ptr(), len(obs_c), 1))
-        pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0)
+        _, ev = pp.evolve_(g, gens, angs, truncation=strat, channel=ch, channel_every=per if ch else 0,
+                           return_expectation=True)
         n_out = len(g)
-        zf = np.empty((n_out, nw), dtype=np.uint64)
-        xf = np.empty((n_out, nw), dtype=np.uint64)
-        cf = np.empty(n_out, dtype=np.float64)
+        if n_out > fcap:                      # (the same circuit every step: not expected)
+            fcap = n_out
+            pz = np.empty((fcap, nw), dtype=np.uint64)
+            px = np.empty((fcap, nw), dtype=np.uint64)
+            pc = np.empty(fcap, dtype=np.float64)
+        zf, xf, cf = pz[:n_out], px[:n_out], pc[:n_out]
         m = pp.spv.c_int64()
         pp.spv.check(pp.spv.lib.pp_download(g._h, zf.ctypes.data, xf.ctypes.data, cf.ctypes.data, n_out,
                                             pp.spv.byref(m)))
-        ev = pp.expectation_value(g, 0)
         te.append(time.perf_counter() - t0)
         h2d = obs_z.nbytes + obs_x.nbytes + obs_c.nbytes + len(gens) * (2 * 8 * nw + 16)
         d2h = zf.nbytes + xf.nbytes + cf.nbytes + 8
