@@ -83,7 +83,6 @@ class GpuShard:
 
     def begin(self, gz, gx, cosv, sinv, opts, bits):
         mx = c_int32(0)
-        self._keep = (gz, gx, cosv, sinv, opts)
         check(lib.pp_shard_begin(self.v._h, self.rank_bits, self.rank, gz.ctypes.data, gx.ctypes.data,
                                  cosv.ctypes.data, sinv.ctypes.data, len(cosv), byref(opts), bits, byref(mx)))
         return mx.value
@@ -153,9 +152,6 @@ class LocalGroup:
 
     def __init__(self, size):
         self.size = size
-
-    def ranks(self, engines):
-        return [e.rank for e in engines]
 
     def exchange(self, engines, sends):
         by_rank = {e.rank: (p, pay) for e, (p, pay) in zip(engines, sends)}
