@@ -134,3 +134,36 @@ def test_shard_config2_layers_with_channel():
     assert len(v) > 10**5
     assert res[4]["bucket_bits"] > 2
     _check(res, v)
+
+
+def test_shard_argument_errors():
+    """Calls out of order or with bad sizes are refused with a status, and the
+    handle stays usable."""
+    import ctypes
+    from pauliprop import _lib
+    N = 64
+    v = pp.SparsePauliVector(N, 64, 16)
+    z, x = pp.pack_keys(N, [(1, 0), (2, 3), (0, 5)])
+    v.upload(z, x, np.array([1.0, 0.5, -0.25]), sorted=False)
+    n, part, st = ctypes.c_int64(), ctypes.c_int32(), np.zeros(5, dtype=np.int64)
+    # no run in progress
+    assert _lib.lib.pp_shard_send(v._h, 0, 0, None, None, None, 0, ctypes.byref(n), ctypes.byref(part)) \
+        == _lib.PP_ARGUMENT_ERROR
+    assert _lib.lib.pp_shard_rotate(v._h, 0, 0, st.ctypes.data) == _lib.PP_ARGUMENT_ERROR
+    assert _lib.lib.pp_shard_end(v._h, None, None) == _lib.PP_ARGUMENT_ERROR
+    # bad rank / bucket bits
+    gz = np.array([[3]], dtype=np.uint64)
+    gx = np.array([[0]], dtype=np.uint64)
+    cs = np.array([0.5]), np.array([0.2])
+    opts = _lib.PPEvolveOpts()
+    opts.window = 1
+    opts.chan_kind = -1
+    mx = ctypes.c_int32()
+    assert _lib.lib.pp_shard_begin(v._h, 1, 2, gz.ctypes.data, gx.ctypes.data, cs[0].ctypes.data, cs[1].ctypes.data,
+                                   1, ctypes.byref(opts), 4, ctypes.byref(mx)) == _lib.PP_ARGUMENT_ERROR
+    assert _lib.lib.pp_shard_begin(v._h, 1, 0, gz.ctypes.data, gx.ctypes.data, cs[0].ctypes.data, cs[1].ctypes.data,
+                                   1, ctypes.byref(opts), 26, ctypes.byref(mx)) == _lib.PP_ARGUMENT_ERROR
+    # the handle still works as a vector
+    assert len(v) == 3
+    pp.check_spv(v)
+    v.close()

@@ -101,3 +101,25 @@ def test_tuning_cache_lookup(tmp_path, monkeypatch):
     assert tune.cached(148, 10, 0, 2) is None
     assert tune.cached(132, 9, 0, 1) is None
     tune._cache.clear()
+
+
+def test_shard_owner_host_side():
+    """pp_shard_owner (host-side): rank_bits GF(2)-linear parities of the key, so
+    owner(P xor M) = owner(P) xor owner(M) for one- and two-word keys, every rank
+    receives keys, and bad arguments are refused."""
+    import numpy as np
+    from pauliprop import _lib, shard
+    rng = np.random.default_rng(3)
+    for nw in (1, 2):
+        z = rng.integers(0, 2**63, size=(4000, nw), dtype=np.uint64)
+        x = rng.integers(0, 2**63, size=(4000, nw), dtype=np.uint64)
+        mz = rng.integers(0, 2**63, size=(1, nw), dtype=np.uint64)
+        mx = rng.integers(0, 2**63, size=(1, nw), dtype=np.uint64)
+        for rb in (0, 1, 3):
+            o = shard.owners(nw, z, x, rb)
+            om = shard.owners(nw, mz, mx, rb)[0]
+            assert np.array_equal(shard.owners(nw, z ^ mz, x ^ mx, rb), o ^ om)
+            assert set(np.unique(o)) == set(range(1 << rb))
+    out = np.zeros(1, dtype=np.int32)
+    assert _lib.lib.pp_shard_owner(3, out.ctypes.data, out.ctypes.data, 1, 1, out.ctypes.data) == _lib.PP_ARGUMENT_ERROR
+    assert _lib.lib.pp_shard_owner(1, out.ctypes.data, out.ctypes.data, 1, 9, out.ctypes.data) == _lib.PP_ARGUMENT_ERROR
