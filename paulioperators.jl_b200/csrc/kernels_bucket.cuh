@@ -201,6 +201,23 @@ __device__ __forceinline__ bool anticommutes(const Key<NW> &p, const GenRec &g) 
     return (m & 1) != 0;
 }
 
+// rotate_term for a P already known to anticommute with G: the sin branch's key
+// P xor M and its phase sign k - 2 (_rotate_range!, spv_kernels.jl:155-163),
+// without the parity test.
+template <int NW>
+__device__ __forceinline__ void rotate_anti(const Key<NW> &p, const GenRec &g, Key<NW> *q, double *sgn) {
+    int m1 = 0, nzp = 0, nzx = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        q->z[w] = g.gz[w] ^ p.z[w];
+        q->x[w] = g.gx[w] ^ p.x[w];
+        m1 += __popcll(g.gx[w] & p.z[w]);
+        nzp += __popcll(q->z[w] & q->x[w]);
+        nzx += __popcll(p.z[w] & p.x[w]);
+    }
+    *sgn = (double)(((nzp - g.ng - nzx + 2 * m1) & 3) - 2);
+}
+
 // Buckets of pair p: (b0, b0 xor delta), or (2p, 2p + 1) when delta = 0.
 __device__ __forceinline__ void bk_pair(unsigned delta, long long p, int *b0, int *b1) {
     if (delta == 0) {
@@ -258,9 +275,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     __shared__ int s_red[3][T / 32];
     extern __shared__ __align__(128) u64 bsm[];
     // staging area a: keys (NW words each, z then x), coefficients; then the key
-    // index and, per area, a byte per staged slot: its local bucket in bits 0-5,
-    // bit 6 for a foreign term (key-sharded runs), bit 7 when the slot holds no
-    // term (a run's padding slot) or one the early merge drops
+    // index and, per area, a byte per staged slot: its local bucket in bits 0-4,
+    // bit 5 once the index pass has found that the term anticommutes with G, bit
+    // 6 for a foreign term (key-sharded runs), bit 7 when the slot holds no term
+    // (a run's padding slot) or one the early merge drops
     constexpr int AREA = (2 * NW + 1) * SMI;       // u64 words of one staging area
     auto skz = [&](int a) { return bsm + a * AREA; };
     auto skx = [&](int a) { return bsm + a * AREA + NW * SMI; };
@@ -452,6 +470,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                 continue;
             }
             if (!anticommutes<NW>(kk, g)) continue;
+            sbk[i] |= 0x20;                  // the rotation pass reads this instead of the parity
             unsigned h = bk_slot<NW, TAB>(kk);
             for (int probe = 0; probe < TAB; ++probe) {
                 if (atomicCAS(&tab[h], (unsigned short)0, (unsigned short)(i + 1)) == (unsigned short)0) break;
@@ -475,7 +494,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             // local bucket (0x7f past the staged terms keeps buckets nondecreasing
             // across the warp) and early-merge drop flag
             const int tag = i < ntot ? sbk[i] : 0x7f;
-            int lb = tag & 0x3f;
+            int lb = tag & 0x1f;
             const bool in = i < ntot && tag < 0x80;
             const bool fgn = (tag & 0x40) != 0;      // a foreign term: its sin branch only
             if (i < ntot && lb >= 2 * (j1 - j0)) {
@@ -484,9 +503,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             }
             bool own = false, nw_ = false;
             double oval = 0.0, nval = 0.0;
+            Key<NW> kk;                  // kept in registers for the stores (no reload after the claims)
             if (in) {
                 alive += fgn ? 0 : 1;
-                const Key<NW> kk = skey(a, i);
+                kk = skey(a, i);
                 const double c = sc(a)[i];
                 double v = c;
                 Key<NW> qk;
@@ -506,7 +526,8 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                         svt = A.bsin[ai];
                     }
                 }
-                if (act && rotate_term<NW>(kk, g, &qk, &sg)) {
+                if (act && (tag & 0x20)) {
+                    rotate_anti<NW>(kk, g, &qk, &sg);
                     v = __dmul_rn(c, cvt);
                     const double s = __dmul_rn(sg * svt, c);     // (k - 2) * sin(theta) * c, spv_kernels.jl:163
                     const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
@@ -543,7 +564,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             if (own) {
                 if (po < CAP) {
                     const long long o = (long long)s_b[a][ob] * CAP + po;
-                    store_key<NW>(OZ, OX, o, skey(a, i));
+                    store_key<NW>(OZ, OX, o, kk);
                     OC[o] = oval;
                 } else {
                     over = true;
@@ -554,7 +575,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
             if (nw_) {
                 if (pn < CAP) {
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
-                    Key<NW> nk = skey(a, i);
+                    Key<NW> nk = kk;
 #pragma unroll
                     for (int w = 0; w < NW; ++w) { nk.z[w] ^= g.gz[w]; nk.x[w] ^= g.gx[w]; }
                     store_key<NW>(OZ, OX, o, nk);
