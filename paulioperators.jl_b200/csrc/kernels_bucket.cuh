@@ -186,15 +186,29 @@ template <int NW>
 __device__ __forceinline__ bool drop_q(const FQuick &q, const DevFilter &f, const Key<NW> &k, double absc) {
     if (q.full) return should_drop<NW>(f, k, absc);
     if (absc <= q.thresh) return true;
-    int wt = 0, xw = 0;
+    int wt = 0;
 #pragma unroll
-    for (int w = 0; w < NW; ++w) { wt += __popcll(k.z[w] | k.x[w]); xw += __popcll(k.x[w]); }
-    return wt > q.wmax || xw > q.xwmax;
+    for (int w = 0; w < NW; ++w) wt += __popcll(k.z[w] | k.x[w]);
+    if (wt > q.wmax) return true;
+    if (q.xwmax >= 64 * NW) return false;        // the X-weight cap cannot drop
+    int xw = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) xw += __popcll(k.x[w]);
+    return xw > q.xwmax;
 }
 
-// P anticommutes with G (the parity test of rotate_term).
+// The generator's key words and popcount(gz & gx), copied to registers by a
+// kernel whose loops also issue shared-memory atomics (after which a GenRec in
+// shared memory would be read again).  anticommutes and rotate_anti take either.
 template <int NW>
-__device__ __forceinline__ bool anticommutes(const Key<NW> &p, const GenRec &g) {
+struct GenKey {
+    u64 gz[NW], gx[NW];
+    int ng;
+};
+
+// P anticommutes with G (the parity test of rotate_term).
+template <int NW, class Gen>
+__device__ __forceinline__ bool anticommutes(const Key<NW> &p, const Gen &g) {
     int m = 0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) m += __popcll(g.gx[w] & p.z[w]) + __popcll(g.gz[w] & p.x[w]);
@@ -204,8 +218,8 @@ __device__ __forceinline__ bool anticommutes(const Key<NW> &p, const GenRec &g) 
 // rotate_term for a P already known to anticommute with G: the sin branch's key
 // P xor M and its phase sign k - 2 (_rotate_range!, spv_kernels.jl:155-163),
 // without the parity test.
-template <int NW>
-__device__ __forceinline__ void rotate_anti(const Key<NW> &p, const GenRec &g, Key<NW> *q, double *sgn) {
+template <int NW, class Gen>
+__device__ __forceinline__ void rotate_anti(const Key<NW> &p, const Gen &g, Key<NW> *q, double *sgn) {
     int m1 = 0, nzp = 0, nzx = 0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
@@ -345,6 +359,10 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
     const bool local_on = P.local_active != 0;
     const FQuick fs = fquick(P.strict);
     const double cv = g.cosv, sv = g.sinv;
+    GenKey<NW> gk;                   // the generator in registers
+#pragma unroll
+    for (int w = 0; w < NW; ++w) { gk.gz[w] = g.gz[w]; gk.gx[w] = g.gx[w]; }
+    gk.ng = g.ng;
     const int flip = delta != 0 ? 1 : 0;
 
     // pair buckets and counts of group gi into area a (threads < G); -1 group: none
@@ -469,7 +487,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                 sbk[i] |= 0x80;
                 continue;
             }
-            if (!anticommutes<NW>(kk, g)) continue;
+            if (!anticommutes<NW>(kk, gk)) continue;
             sbk[i] |= 0x20;                  // the rotation pass reads this instead of the parity
             unsigned h = bk_slot<NW, TAB>(kk);
             for (int probe = 0; probe < TAB; ++probe) {
@@ -527,7 +545,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     }
                 }
                 if (act && (tag & 0x20)) {
-                    rotate_anti<NW>(kk, g, &qk, &sg);
+                    rotate_anti<NW>(kk, gk, &qk, &sg);
                     v = __dmul_rn(c, cvt);
                     const double s = __dmul_rn(sg * svt, c);     // (k - 2) * sin(theta) * c, spv_kernels.jl:163
                     const bool s_ok = !(local_on && should_drop<NW>(P.local, qk, fabs(s)));
@@ -577,7 +595,7 @@ __global__ void __launch_bounds__(BK_THREADS, bk_min_blocks(NW, ITEMS)) k_bk_rot
                     const long long o = (long long)s_b[a][tb] * CAP + pn;
                     Key<NW> nk = kk;
 #pragma unroll
-                    for (int w = 0; w < NW; ++w) { nk.z[w] ^= g.gz[w]; nk.x[w] ^= g.gx[w]; }
+                    for (int w = 0; w < NW; ++w) { nk.z[w] ^= gk.gz[w]; nk.x[w] ^= gk.gx[w]; }
                     store_key<NW>(OZ, OX, o, nk);
                     OC[o] = nval;
                 } else {
