@@ -15,6 +15,7 @@ Term arrays stay in device memory between calls.
 """
 import ctypes
 import math
+import operator
 from ctypes import byref, c_double, c_int32, c_int64, c_void_p
 
 import numpy as np
@@ -188,13 +189,28 @@ def PauliSum_from(v):
     return v.to_paulisum()
 
 
+_get_z, _get_x = operator.attrgetter("z"), operator.attrgetter("x")
+
+
 def _gen_words(N, generators):
     nw = nwords(N)
     L = len(generators)
     if nw == 1:
-        gz = np.fromiter((g.z if type(g) is PauliBasis else int(g[0]) for g in generators), np.uint64, L)
-        gx = np.fromiter((g.x if type(g) is PauliBasis else int(g[1]) for g in generators), np.uint64, L)
+        try:                        # all PauliBasis (the usual case): no per-item type test
+            gz = np.fromiter(map(_get_z, generators), np.uint64, L)
+            gx = np.fromiter(map(_get_x, generators), np.uint64, L)
+        except AttributeError:      # (z, x) pairs among them
+            gz = np.fromiter((g.z if type(g) is PauliBasis else int(g[0]) for g in generators), np.uint64, L)
+            gx = np.fromiter((g.x if type(g) is PauliBasis else int(g[1]) for g in generators), np.uint64, L)
         return gz.reshape(L, 1), gx.reshape(L, 1)
+    nb = 8 * nw
+    try:                            # all PauliBasis with in-range words: little-endian bytes of each int
+        bz = b"".join([z.to_bytes(nb, "little") for z in map(_get_z, generators)])
+        bx = b"".join([x.to_bytes(nb, "little") for x in map(_get_x, generators)])
+        return (np.frombuffer(bz, dtype="<u8").reshape(L, nw).astype(np.uint64),
+                np.frombuffer(bx, dtype="<u8").reshape(L, nw).astype(np.uint64))
+    except (AttributeError, OverflowError):
+        pass                        # (z, x) pairs, or words beyond nw * 64 bits (masked below)
     m = (1 << 64) - 1
     zs = [g.z if isinstance(g, PauliBasis) else int(g[0]) for g in generators]
     xs = [g.x if isinstance(g, PauliBasis) else int(g[1]) for g in generators]
@@ -204,6 +220,25 @@ def _gen_words(N, generators):
         gz[:, w] = np.fromiter(((z >> (64 * w)) & m for z in zs), dtype=np.uint64, count=L)
         gx[:, w] = np.fromiter(((x >> (64 * w)) & m for x in xs), dtype=np.uint64, count=L)
     return gz, gx
+
+
+def _cos_sin(angles):
+    """cos θ and sin θ of every angle from the host's libm (math.cos / math.sin,
+    as the reference computes them on its host, spv_evolve.jl:341-342), each
+    evaluated once per distinct angle: a circuit of repeated layers has few.
+    Angles are told apart by their bit patterns, so -0.0 and 0.0 (whose sines
+    differ in sign) and NaN payloads are kept apart."""
+    ang = angles if isinstance(angles, np.ndarray) else np.fromiter(angles, np.float64, len(angles))
+    ang = np.ascontiguousarray(ang, dtype=np.float64)
+    if len(ang) <= 16:
+        al = ang.tolist()
+        return (np.fromiter(map(math.cos, al), np.float64, len(al)),
+                np.fromiter(map(math.sin, al), np.float64, len(al)))
+    u, inv = np.unique(ang.view(np.uint64), return_inverse=True)
+    ul = u.view(np.float64).tolist()
+    cu = np.fromiter(map(math.cos, ul), np.float64, len(ul))
+    su = np.fromiter(map(math.sin, ul), np.float64, len(ul))
+    return cu[inv], su[inv]
 
 
 def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=None,
@@ -293,11 +328,8 @@ def evolve_(v, G, theta=None, *, window=1, truncation=None, local_truncation=Non
     opts.stats_out = st.ctypes.data_as(ctypes.POINTER(c_double))
     opts.profile = 1 if profile else 0
     gz, gx = _gen_words(v.N, generators)
-    ang = np.asarray(angles, dtype=np.float64)
-    al = ang.tolist()
-    cosv = np.fromiter(map(math.cos, al), np.float64, len(al))     # libm, as the reference's host
-    sinv = np.fromiter(map(math.sin, al), np.float64, len(al))
-    check(lib.pp_evolve(v._h, _ptr(gz), _ptr(gx), _ptr(cosv), _ptr(sinv), len(ang), byref(opts)))
+    cosv, sinv = _cos_sin(angles)
+    check(lib.pp_evolve(v._h, _ptr(gz), _ptr(gx), _ptr(cosv), _ptr(sinv), len(cosv), byref(opts)))
     if isinstance(correction, (EnergyCorrection, EnergyVarianceCorrection)):
         correction.accumulated_energy = ce.value
     if isinstance(correction, EnergyVarianceCorrection):

@@ -123,3 +123,52 @@ def test_shard_owner_host_side():
     out = np.zeros(1, dtype=np.int32)
     assert _lib.lib.pp_shard_owner(3, out.ctypes.data, out.ctypes.data, 1, 1, out.ctypes.data) == _lib.PP_ARGUMENT_ERROR
     assert _lib.lib.pp_shard_owner(1, out.ctypes.data, out.ctypes.data, 1, 9, out.ctypes.data) == _lib.PP_ARGUMENT_ERROR
+
+
+def test_generator_words_and_angles_host_side():
+    """evolve_'s host packing of generators into little-endian key words and its
+    cos/sin of the angles (libm once per distinct angle bit pattern) equal a
+    per-element restatement bit for bit: one- and two-word keys, (z, x) pairs
+    mixed with PauliBasis, words beyond the key width (masked for two-word keys,
+    refused for one-word keys), -0.0 against 0.0, NaN, subnormals.  No GPU
+    call."""
+    import random
+    import numpy as np
+    from pauliprop import spv
+    from pauliprop.paulis import PauliBasis
+
+    def words(N, gens):
+        nw = pp.nwords(N)
+        m = (1 << 64) - 1
+        zs = [g.z if isinstance(g, PauliBasis) else int(g[0]) for g in gens]
+        xs = [g.x if isinstance(g, PauliBasis) else int(g[1]) for g in gens]
+        gz = np.array([[(z >> (64 * w)) & m for w in range(nw)] for z in zs], dtype=np.uint64).reshape(len(gens), nw)
+        gx = np.array([[(x >> (64 * w)) & m for w in range(nw)] for x in xs], dtype=np.uint64).reshape(len(gens), nw)
+        return gz, gx
+
+    rng = random.Random(7)
+    for N in (1, 20, 64, 65, 127, 128):
+        m = (1 << N) - 1
+        for L in (0, 1, 40, 700):
+            gens = [PauliBasis(N, rng.getrandbits(N) & m, rng.getrandbits(N) & m) for _ in range(L)]
+            cases = [gens, [((g.z, g.x) if i % 3 == 0 else g) for i, g in enumerate(gens)]]
+            big = gens[:-1] + [PauliBasis(N, 1 << (64 * pp.nwords(N) + 3), 5)]
+            if L and pp.nwords(N) > 1:
+                cases.append(big)           # masked to the key width, as before
+            elif L:
+                with pytest.raises(OverflowError):
+                    spv._gen_words(N, big)  # a one-word key does not fit: refused, as before
+            for g2 in cases:
+                a, b = words(N, g2), spv._gen_words(N, g2)
+                for p, q in zip(a, b):
+                    assert q.dtype == np.uint64 and q.shape == p.shape and np.array_equal(p, q)
+    base = [0.3, -1.1, 2.5, 0.0, -0.0, float("nan"), 5e-324, -1e-300]
+    for L in (0, 3, 16, 17, 400):
+        for angles in ([rng.choice(base) for _ in range(L)], [rng.uniform(-4, 4) for _ in range(L)],
+                       np.array([rng.choice(base) for _ in range(L)], dtype=np.float32)):
+            c, s = spv._cos_sin(angles)
+            al = np.asarray(angles, dtype=np.float64).tolist()
+            assert np.array_equal(c.view(np.uint64), np.array([math.cos(a) for a in al], dtype=np.float64).view(np.uint64))
+            assert np.array_equal(s.view(np.uint64), np.array([math.sin(a) for a in al], dtype=np.float64).view(np.uint64))
+    with pytest.raises(ValueError):
+        spv._cos_sin([0.5] * 20 + [float("inf")])
