@@ -27,7 +27,6 @@ or one process driving several GPUs) or one rank per process (DistGroup over
 torch.distributed, NCCL between GPUs).
 """
 import ctypes
-import math
 
 import numpy as np
 
@@ -36,7 +35,7 @@ from ctypes import byref, c_double, c_int32, c_int64
 from . import _lib
 from ._lib import PPEvolveOpts, check, lib
 from .errors import ArgumentError
-from .paulis import PauliBasis, nwords, pack_word, qubit_mask
+from .paulis import pack_word, qubit_mask
 from .truncation import NoTruncation, compile_filter, is_compilable
 
 
@@ -138,13 +137,13 @@ class GpuShard:
 
 
 def _settle(payloads):
-    """The copies into received payloads (made on torch's stream) are complete
-    before an engine's own stream reads them."""
-    for p in payloads:
-        if p is not None and p[2].is_cuda:
-            import torch
-            torch.cuda.current_stream(p[2].device).synchronize()
-            return
+    """The copies into received payloads (made on torch's current stream of each
+    payload's device) are complete before an engine's own stream reads them."""
+    devices = {p[2].device for p in payloads if p is not None and p[2].is_cuda}
+    if devices:
+        import torch
+        for d in devices:
+            torch.cuda.current_stream(d).synchronize()
 
 
 class LocalGroup:
@@ -162,7 +161,8 @@ class LocalGroup:
             else:
                 p2, pay = by_rank[partner]
                 assert p2 == e.rank, "partner ranks must pair up"
-                out.append(tuple(t.clone() for t in pay))
+                dev = getattr(e, "dev", None)     # the receiving rank's device (engines on several GPUs)
+                out.append(tuple(t.clone() if dev is None else t.to(dev, copy=True) for t in pay))
         _settle(out)
         return out
 
@@ -210,14 +210,11 @@ class DistGroup:
         return t.item()
 
 
-def _gen_arrays(nw, generators, angles):
-    zs = [g.z if isinstance(g, PauliBasis) else int(g[0]) for g in generators]
-    xs = [g.x if isinstance(g, PauliBasis) else int(g[1]) for g in generators]
-    m = (1 << 64) - 1
-    gz = np.array([[(z >> (64 * w)) & m for w in range(nw)] for z in zs], dtype=np.uint64).reshape(-1, nw)
-    gx = np.array([[(x >> (64 * w)) & m for w in range(nw)] for x in xs], dtype=np.uint64).reshape(-1, nw)
-    cosv = np.array([math.cos(a) for a in angles], dtype=np.float64)
-    sinv = np.array([math.sin(a) for a in angles], dtype=np.float64)
+def _gen_arrays(N, generators, angles):
+    """Generator key words and libm cos / sin of the angles, prepared as evolve_ does."""
+    from .spv import _cos_sin, _gen_words
+    gz, gx = _gen_words(N, generators)
+    cosv, sinv = _cos_sin(angles)
     return gz, gx, cosv, sinv
 
 
@@ -237,7 +234,6 @@ def run_sharded(engines, group, N, generators, angles, *, truncation=None, local
     if not (is_compilable(truncation) and is_compilable(local_truncation)):
         raise NotImplementedError("key-sharded runs take compiled (coefficient / weight) truncations")
     L = len(generators)
-    nw = nwords(N)
     opts = PPEvolveOpts()
     opts.window = 1
     strict_f = _pp_filter(compile_filter(truncation))
@@ -258,7 +254,7 @@ def run_sharded(engines, group, N, generators, angles, *, truncation=None, local
         mask_w = pack_word(N, qubit_mask(N, qubits))
         opts.chan_mask = mask_w.ctypes.data
     opts.chan_every = int(channel_every or 0)
-    gz, gx, cosv, sinv = _gen_arrays(nw, generators, angles)
+    gz, gx, cosv, sinv = _gen_arrays(N, generators, angles)
     caps = {e.tuning()[0] for e in engines}
     if len(caps) != 1:
         raise ArgumentError("every rank needs the same bucket capacity")

@@ -24,10 +24,9 @@ from . import _lib
 from ._lib import (ArgumentError, DimensionMismatch, PPCounters, PPEvolveOpts, PPFilter,
                    check, lib)
 from .paulis import PauliBasis, PauliSum, nwords, pack_keys, pack_word, qubit_mask, unpack_keys
-from .truncation import (NOFILTER, AdaptiveTruncation, CompositeTruncation, CorrectionAccumulator,
-                         EnergyCorrection, EnergyVarianceCorrection, NoCorrection, NoTruncation,
-                         StochasticCoeffTruncation, StochasticSamplingTruncation, compile_filter,
-                         draw_seed, is_compilable)
+from .truncation import (AdaptiveTruncation, CompositeTruncation, EnergyCorrection, EnergyVarianceCorrection,
+                         NoCorrection, NoTruncation, StochasticCoeffTruncation, StochasticSamplingTruncation,
+                         compile_filter, draw_seed, is_compilable)
 
 CHANNEL_KINDS = {"depolarizing": 0, "dephasing": 1, "bit_flip": 2, "bit_phase_flip": 3, "pauli": 4}
 

@@ -177,6 +177,49 @@ def _worker(rank, ws, port, q, seed, acap):
         q.put(("error", traceback.format_exc(), repr(ex), None))
 
 
+def _oracle_terms(seed, acap):
+    sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")]
+    import orc
+    from helpers import filt
+    terms, gens, angs = _case(seed)
+    v = orc.OracleSPV(40, max(16, 2 * len(terms)), acap)
+    v.upload([k[0] for k in terms], [k[1] for k in terms], list(terms.values()))
+    v.evolve(gens, angs, window=1, strict=filt(("comp", [("coeff", 1e-2), ("weight", 12)])))
+    oz, ox, oc = v.arrays()
+    ref = {(int(oz[i, 0]), int(ox[i, 0])): float(oc[i]) for i in range(len(oc))}
+    diag = ox[:, 0] == 0
+    return ref, v.expect(0), float(abs(oc[diag]).sum())
+
+
+@pytest.mark.parametrize("acap", [1 << 20, 40])
+def test_sharded_protocol_local_group(acap):
+    """The same protocol with both ranks in this process (LocalGroup: the
+    exchange is a copy between the engines, as for virtual ranks on one GPU)."""
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "paulioperators.jl_b200")]
+    import numpy as np
+    from pauliprop import shard
+    from pauliprop.truncation import CoeffTruncation, CompositeTruncation, WeightTruncation
+    seed = 21
+    terms, gens, angs = _case(seed)
+    keys = list(terms)
+    z = np.array([[k[0]] for k in keys], dtype=np.uint64)
+    x = np.array([[k[1]] for k in keys], dtype=np.uint64)
+    own = shard.owners(1, z, x, 1)
+    engines = [FakeShard(40, {k: terms[k] for k, o in zip(keys, own) if o == r}, 1, r, 1e-2, 12) for r in range(2)]
+    strat = CompositeTruncation(CoeffTruncation(1e-2), WeightTruncation(12))
+    e, st = shard.run_sharded(engines, shard.LocalGroup(2), 40, gens, angs, truncation=strat, append_capacity=acap)
+    union = {}
+    for eng in engines:
+        assert not (set(eng.L) & set(union))
+        union.update(eng.L)
+    ref, ev, scale = _oracle_terms(seed, acap)
+    assert len(union) == len(ref) > 0 and set(union) == set(ref), "key sets differ"
+    assert all(union[k] == ref[k] for k in ref), "coefficients differ"
+    assert abs(e - ev) <= 1e-12 * max(1e-300, scale)
+    if acap == 40:
+        assert st["append_capacity"] > 40
+
+
 @pytest.mark.parametrize("acap", [1 << 20, 40])
 def test_sharded_protocol_two_gloo_ranks(acap):
     """acap 2^20: no early merge; acap 40: the global count passes it, so the
