@@ -1620,7 +1620,7 @@ struct Scratch {
         void *q = nullptr;
         if (cudaMalloc(&q, (size_t)std::max(1ll, count) * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
-            return fail(PP_OUT_OF_MEMORY, "cudaMalloc (stochastic truncation scratch)");
+            return fail(PP_OUT_OF_MEMORY, "cudaMalloc (scratch buffer)");
         }
         p.push_back(q);
         *out = (T *)q;
@@ -2998,6 +2998,7 @@ extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *c
     k_sel_scan<<<1, 1024, 0, s>>>(ntiles, m->sel, m->cgt, m->ceq, m->tie_off, m->out_off, m->total);
     k_sel_write<<<g, SL_THREADS, 0, s>>>(m->score, n, m->sel, m->tie_off, m->out_off, h->z[cur], h->x[cur], h->c[cur],
                                          h->z[cur ^ 1], h->x[cur ^ 1], h->c[cur ^ 1]);
+    Scratch sample_buf;             // the drop sample's device buffer, freed on every return
     u64 *sbuf = nullptr;
     unsigned long long *scnt = nullptr;
     long long scap = sample ? sample->cap : 0;
@@ -3006,7 +3007,7 @@ extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *c
         const double pacc = std::min(1.0, 0.9 * (double)scap / (double)(n - budget));
         const unsigned long long thr =
             pacc >= 1.0 ? ~0ull : (unsigned long long)(pacc * 18446744073709551616.0);
-        CU(cudaMalloc((void **)&sbuf, (size_t)scap * 24 + 8));
+        TRY(sample_buf.get(&sbuf, 3 * scap + 1));     // z, x, c words of the sample, then its counter
         scnt = reinterpret_cast<unsigned long long *>(sbuf + 3 * scap);
         CU(cudaMemsetAsync(scnt, 0, 8, s));
         k_sel_sample<<<h->nsm * 4, 256, 0, s>>>(m->score, n, m->sel, sample->seed, thr, h->z[cur], h->x[cur],
@@ -3026,7 +3027,6 @@ extern "C" int pp_learned_truncate(pp_spv *h, pp_mlp *m, const pp_feature_ctx *c
         cudaMemcpy(sample->z, sbuf, ns * 8, cudaMemcpyDefault);
         cudaMemcpy(sample->x, sbuf + scap, ns * 8, cudaMemcpyDefault);
         cudaMemcpy(sample->c, sbuf + 2 * scap, ns * 8, cudaMemcpyDefault);
-        cudaFree(sbuf);
         sample->n = ns;
     }
     int e = 0;

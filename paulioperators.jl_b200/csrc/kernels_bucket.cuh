@@ -788,8 +788,7 @@ __host__ __device__ __forceinline__ unsigned bk_owner(const u64 *kz, const u64 *
     for (int k = 0; k < rank_bits; ++k) {
         const u64 *R = rows + 4 * (BK_ROWS - 1 - k);
         int p = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) p += popc64(kz[w] & R[w]) + popc64(kx[w] & R[2 + w]);
+        for (int w = 0; w < NW; ++w) p += popc64(kz[w] & R[w]) + popc64(kx[w] & R[2 + w]);   // NW: 1 or 2
         o |= (unsigned)(p & 1) << k;
     }
     return o;
