@@ -172,3 +172,40 @@ def test_generator_words_and_angles_host_side():
             assert np.array_equal(s.view(np.uint64), np.array([math.sin(a) for a in al], dtype=np.float64).view(np.uint64))
     with pytest.raises(ValueError):
         spv._cos_sin([0.5] * 20 + [float("inf")])
+
+
+def test_batch_tags_and_shard_split_host_side():
+    """Host helpers around the device calls: tagged_terms / split_instances
+    round-trip each instance's terms (instance index in z word 1); shard.split
+    partitions a term set exactly by owner; bits_for gives the fewest bucket
+    bits whose mean load stays within cap / load_div.  No GPU call."""
+    import random
+    import numpy as np
+    from pauliprop import shard
+    from pauliprop.batch import split_instances, tagged_terms
+
+    rng = random.Random(3)
+    obs = [[(rng.getrandbits(64), rng.getrandbits(64), rng.uniform(-1, 1)) for _ in range(rng.randrange(0, 7))]
+           for _ in range(5)]
+    z, x, c = tagged_terms(obs)
+    assert z.shape == (sum(map(len, obs)), 2) and np.array_equal(np.unique(z[:, 1]), [i for i, o in enumerate(obs) if o])
+    for i, (pz, px, pc) in enumerate(split_instances(z, x, c, len(obs))):
+        assert [(int(a), int(b), float(v)) for a, b, v in zip(pz, px, pc)] == obs[i]
+
+    for nw, rank_bits in ((1, 1), (1, 3), (2, 2)):
+        n = 500
+        z = np.array([[rng.getrandbits(64) for _ in range(nw)] for _ in range(n)], dtype=np.uint64)
+        x = np.array([[rng.getrandbits(64) for _ in range(nw)] for _ in range(n)], dtype=np.uint64)
+        c = np.arange(n, dtype=np.float64)
+        parts = shard.split(nw, z, x, c, rank_bits)
+        assert len(parts) == 1 << rank_bits
+        assert sorted(np.concatenate([p[2] for p in parts]).tolist()) == c.tolist()
+        for r, (pz, px, pc) in enumerate(parts):
+            assert np.all(shard.owners(nw, pz, px, rank_bits) == r)
+            assert np.array_equal(pz, z[pc.astype(int)]) and np.array_equal(px, x[pc.astype(int)])
+
+    for n in (0, 1, 1000, 10**6, 10**9):
+        b = shard.bits_for(n, 512, 6)
+        assert 1 <= b <= 26
+        assert b == 26 or (512 << b) >= 6 * n
+        assert b == 1 or (512 << (b - 1)) < 6 * n
